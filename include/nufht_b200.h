@@ -1,0 +1,226 @@
+/*
+ * nufht_b200.h -- C ABI of the B200 batched nonuniform fast Hankel transform.
+ *
+ *   g[i, t] = sum_j c[j, t] * J_nu(k_i * r_j),   i < n targets, j < m sources, t < batch.
+ *
+ * Part 1 re-declares, with identical names, struct layouts, argument meaning and
+ * return codes, the public interface of the reference library Ansal06/NUFHT
+ * (src/fast_hankel_nufht.h).  A program compiled against the reference header links
+ * against libnufht_b200.so unchanged; every transform then runs on the GPU.
+ * Pointers passed to Part 1 may be host or device pointers (detected per call).
+ *
+ * Part 2 is this library's own extension: a device-resident plan, explicit CUDA
+ * streams, device pointers and precision selection.
+ *
+ * Deliberate deviations from the reference (each one also has a test):
+ *   - inputs rs and ws must be finite, non-negative and non-decreasing; the reference
+ *     assumes this without checking (src/fast_hankel_nufht.c:454-466).  Violations
+ *     return NUFHT_E_UNSORTED_RS / NUFHT_E_UNSORTED_WS from nufht_plan_init.
+ *   - for odd integer nu < 0 the sign (-1)^nu is applied exactly once for every batch
+ *     size (the reference applies it twice when batch == 1,
+ *     src/fast_hankel_nufht.c:916-920 and :1090-1095);
+ *   - the all-direct path (m*n < min_dim_prod) evaluates J_|nu| like every other path
+ *     (the reference hands the signed nu to GSL there, src/fast_hankel_nufht.c:1049).
+ */
+#ifndef NUFHT_B200_H
+#define NUFHT_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ======================= Part 1: reference-compatible ABI ======================= */
+
+/* Replaces NufhtOptions, src/fast_hankel_nufht.h:21-28 (same layout). */
+typedef struct {
+    double tol;          /* default 1e-8 */
+    int    max_levels;   /* <= 0: floor(log2(min(m,n)^2 / min_dim_prod)) */
+    int    min_dim_prod; /* default 10000 */
+    double z_split;      /* NaN: from the tables */
+    int    K_asy;        /* <= 0: from the tolerance formula */
+    int    K_loc;        /* <= 0: from the tables */
+} NufhtOptions;
+
+/* Replaces nufht_default_options, src/fast_hankel_nufht.h:31. */
+NufhtOptions nufht_default_options(void);
+
+/* Replaces Box / BoxVector / Boxes, src/fast_hankel_nufht.h:35-55 (same layouts).
+ * i indexes targets (ws), j indexes sources (rs); bounds are inclusive. */
+typedef struct { int i0, i1; int j0, j1; } Box;
+typedef struct { Box *data; size_t length; size_t capacity; } BoxVector;
+typedef struct { BoxVector loc; BoxVector asy; BoxVector dir; } Boxes;
+
+/* Replaces boxes_free, src/fast_hankel_nufht.h:59. */
+void boxes_free(Boxes *boxes);
+
+/* Replaces NufhtPlan, src/fast_hankel_nufht.h:64-83 (same layout).  The GPU state of
+ * a plan (device copies of rs/ws, work lists, FFT plans, workspace) is kept by the
+ * library, keyed by the plan's address, and released by nufht_plan_free. */
+typedef struct {
+    double nu;
+    double tol;
+    double z_split;
+    int    K_asy;
+    int    K_loc;
+    double asy_coef[64];
+    int m;
+    int n;
+    const double *rs;
+    const double *ws;
+    int max_levels;
+    int min_dim_prod;
+    Boxes boxes;
+    int tables_loaded;
+} NufhtPlan;
+
+/* Replaces NufhtScratch, src/fast_hankel_nufht.h:86-101 (same layout).  The buffers are
+ * allocated with the reference's sizes for ABI compatibility; GPU execution keeps its
+ * own device workspace inside the plan state. */
+typedef struct {
+    double *in_buffer;
+    double *out_buffer;
+    double *real_buffer_1;
+    double *real_buffer_2;
+    double *cheb_buffer;
+    double *bessel_buffer_1;
+    double *bessel_buffer_2;
+    int m_alloc;
+    int n_alloc;
+    int Kloc_alloc;
+    int extra_alloc;
+} NufhtScratch;
+
+/* Replaces nufht_plan_init, src/fast_hankel_nufht.h:106-111 / .c:759-786.
+ * Returns 0, or -1..-6 (parameter errors as the reference), -200 (NULL / empty),
+ * NUFHT_E_UNSORTED_RS, NUFHT_E_UNSORTED_WS. */
+int nufht_plan_init(NufhtPlan *plan, double nu, const double *rs, int m, const double *ws,
+                    int n, const NufhtOptions *opt);
+
+/* Replaces nufht_plan_free, src/fast_hankel_nufht.h:114. */
+void nufht_plan_free(NufhtPlan *plan);
+
+/* Replaces nufht_scratch_init / nufht_scratch_free, src/fast_hankel_nufht.h:117-119.
+ * Returns 0, -300 (NULL), -301 (allocation failure). */
+int nufht_scratch_init(NufhtScratch *scratch, const NufhtPlan *plan);
+void nufht_scratch_free(NufhtScratch *scratch);
+
+/* Replaces generate_boxes, src/fast_hankel_nufht.h:128-134 / .c:578-744 (same boxes,
+ * found by binary search instead of a linear scan). */
+Boxes generate_boxes(const double *rs, int m, const double *ws, int n, double z_split,
+                     int max_levels, int min_dim_prod, int K_loc_threshold);
+
+/* Replaces split_box, src/fast_hankel_nufht.h:138-144 / .c:523-574. */
+void split_box(const double *rs, int m, const double *ws, int n, const Box *box, double z,
+               int *ispl_out, int *jspl_out);
+
+/* Replaces nufht_batch, src/fast_hankel_nufht.h:155-160 / .c:989-1107.
+ * cs: m x batch column-major, leading dimension ld_cs >= m; gs: n x batch, ld_gs >= n,
+ * overwritten.  Host or device pointers.  scratch may be NULL.
+ * Returns 0, -400 (bad args), -401 (leading dims), or NUFHT_E_CUDA / NUFHT_E_NO_DEVICE. */
+int nufht_batch(const NufhtPlan *plan, const double *cs, int ld_cs, double *gs, int ld_gs,
+                int batch, NufhtScratch *scratch);
+
+/* Replaces nufht_inplace and nufht, src/fast_hankel_nufht.h:163-177 / .c:1111-1159.
+ * On failure they print to stderr and leave gs zeroed, as the reference does. */
+void nufht_inplace(double *gs, double nu, const double *rs, int m, const double *cs,
+                   const double *ws, int n, const NufhtOptions *opt);
+double *nufht(double nu, const double *rs, int m, const double *cs, const double *ws, int n,
+              const NufhtOptions *opt);
+
+/* Replaces generate_tables, src/fast_hankel_nufht.h:181 / src/bounds.c:306-324: fills the
+ * library's planning tables from their defining formulas. */
+void generate_tables(void);
+
+/* Replace the evaluators of src/fast_hankel_nufht.h:185-238 (src/expansions.c).  Each
+ * adds one box's contribution to gs on the GPU.  Host or device pointers.  The
+ * scratch-buffer arguments are accepted for ABI compatibility and not used. */
+void add_dir(double *gs, double nu, const double *rs, const double *cs, const double *ws,
+             int m, int n);
+void add_dir_batch(double *gs, double nu, const double *rs, const double *cs,
+                   const double *ws, int m, int n, int batch, int ld_cs, int ld_gs);
+void add_asy(double *gs, double nu, const double *rs, const double *cs, const double *ws,
+             int m, int n, int K, double tol, const double *asy_coef, double *real_buffer_1,
+             double *real_buffer_2, double *in_buffer, double *out_buffer);
+void add_asy_batch(double *gs, double nu, const double *rs, const double *cs,
+                   const double *ws, int m, int n, int K, double tol, const double *asy_coef,
+                   int batch, int ld_cs, int ld_gs, double *in_buffer, double *out_buffer);
+void add_loc(double *gs, double nu, const double *rs, const double *cs, const double *ws,
+             int m, int n, int K, double *cheb_buffer, double *bessel_buffer_1,
+             double *bessel_buffer_2);
+void add_loc_batch(double *gs, double nu, const double *rs, const double *cs,
+                   const double *ws, int m, int n, int K, int batch, int ld_cs, int ld_gs,
+                   double *cheb_buffer_batch, double *bessel_buffer_1, double *bessel_buffer_2);
+
+/* ======================= Part 2: B200 extension ======================= */
+
+/* Error codes added by this library (the reference's codes are kept as they are). */
+#define NUFHT_E_UNSORTED_RS  (-410) /* rs not finite, non-negative and non-decreasing */
+#define NUFHT_E_UNSORTED_WS  (-411) /* ws not finite, non-negative and non-decreasing */
+#define NUFHT_E_CUDA         (-420) /* a CUDA runtime or cuFFT call failed */
+#define NUFHT_E_NO_DEVICE    (-422) /* no CUDA device */
+#define NUFHT_E_TOO_LARGE    (-423) /* sizes exceed what this entry point accepts */
+#define NUFHT_E_BAD_FLAGS    (-424) /* unknown flag bits */
+
+/* Plan flags. */
+#define NUFHT_B200_FP64            0x0   /* all arithmetic in FP64 (default) */
+#define NUFHT_B200_MIXED           0x1   /* mixed precision (FP32 storage / split products) */
+#define NUFHT_B200_EXTENDED_TABLES 0x10  /* fill the asymptotic table at K_asy = 10, which the
+                                            reference leaves empty (affects |nu| >= 35) */
+
+typedef struct NufhtDevicePlan NufhtDevicePlan;
+
+/* Summary of a device plan. */
+typedef struct {
+    double nu, tol, z_split;
+    int K_asy, K_loc;
+    long n_loc, n_asy, n_dir;      /* box counts */
+    long fft_points;               /* sum over asymptotic boxes of the FFT length */
+    int spread_width;              /* exponential-of-semicircle kernel width */
+    int path;                      /* 0 boxes, 1 all-direct, 2 all-asymptotic (half-integer) */
+    size_t workspace_bytes;        /* device workspace for the last batch size executed */
+} NufhtB200Info;
+
+/* Build a device plan.  rs (m) and ws (n) may be host or device pointers; they are
+ * copied, so the caller may free them afterwards.  device: CUDA ordinal.
+ * Returns 0 or a negative code (same codes as nufht_plan_init, plus Part 2 codes). */
+int nufht_b200_plan_create(NufhtDevicePlan **out, double nu, const double *rs, int m,
+                           const double *ws, int n, const NufhtOptions *opt, int flags,
+                           int device);
+
+/* g = H c on `stream` (a cudaStream_t; NULL = legacy default stream).  cs and gs are
+ * DEVICE pointers; column-major with leading dimensions ld_cs >= m, ld_gs >= n.  The call
+ * is asynchronous with respect to the host. */
+int nufht_b200_execute(NufhtDevicePlan *plan, const double *cs, int ld_cs, double *gs,
+                       int ld_gs, int batch, void *stream);
+
+int nufht_b200_plan_info(const NufhtDevicePlan *plan, NufhtB200Info *info);
+void nufht_b200_plan_destroy(NufhtDevicePlan *plan);
+
+/* Copy the plan's boxes (4 ints each, loc then asy then dir) into out (cap boxes).
+ * Returns the total number of boxes. */
+long nufht_b200_plan_boxes(const NufhtDevicePlan *plan, int *out, long cap);
+
+/* Human-readable text for any code returned by this library. */
+const char *nufht_b200_strerror(int code);
+
+/* Number of kernel launches made by this library in the calling process so far. */
+long long nufht_b200_launch_count(void);
+
+/* Device-side Bessel function values J_nu(x[i]) for nu integer (|nu| <= 200) or
+ * half-integer (|nu| <= 19/2); x and out are device pointers.  Exposed for testing the
+ * device special-function code. */
+int nufht_b200_besselj(double nu, const double *x, double *out, long count, void *stream);
+
+/* Where the planning tables were read from (a cache file path), or "generated". */
+const char *nufht_b200_table_source(void);
+
+/* Generate the planning tables from their formulas and write them to `path` in the
+ * reference's cache format.  Returns 0 on success. */
+int nufht_b200_write_tables(const char *path);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NUFHT_B200_H */

@@ -1,0 +1,83 @@
+"""Drop-in for the reference's Python extension module `_pynufht` (src/_pynufht.c).
+
+Same three functions, argument meaning, result layout and exceptions:
+
+  nufht(nu, rs, cs, ws, tol=1e-8)            -> ndarray (n,)
+  nufht_batch(nu, rs, cs, ws, tol=1e-8)      -> ndarray (n, batch), C order
+  nufht_batch_loop(nu, rs, cs, ws, tol=1e-8) -> ndarray (n, batch), one transform per column
+
+Each call plans (on the host) and runs the transform on the GPU through the C ABI of
+libnufht_b200.so, as the reference plans and runs on the CPU per call (src/_pynufht.c:186).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+
+__all__ = ["nufht", "nufht_batch", "nufht_batch_loop"]
+
+
+def _vec(a):
+    return L.as_f64(a, "C").ravel() if np.ndim(a) != 1 else L.as_f64(a, "C")
+
+
+def nufht(nu, rs, cs, ws, tol=1e-8):
+    """Single transform via the C entry point nufht() (src/_pynufht.c:17-62)."""
+    lib = L.lib()
+    rs = _vec(rs)
+    ws = _vec(ws)
+    cs = L.as_f64(cs, "C")
+    m, n = rs.shape[0], ws.shape[0]
+    opt = L.options(tol=float(tol))
+    out = lib.nufht(float(nu), L.dptr(rs), m, L.dptr(cs), L.dptr(ws), n, ctypes.byref(opt))
+    if not out:
+        raise RuntimeError("nufht returned NULL")
+    try:
+        res = np.ctypeslib.as_array(ctypes.cast(out, ctypes.POINTER(ctypes.c_double)), shape=(n,)).copy()
+    finally:
+        ctypes.CDLL(None).free(ctypes.c_void_p(out))
+    return res
+
+
+def _check_batch(rs, cs):
+    cs = np.asarray(cs, dtype=np.float64)
+    if cs.ndim != 2:
+        raise ValueError("cs must be 2-D array with shape (m, batch)")
+    if cs.shape[0] != rs.shape[0]:
+        raise ValueError("cs first dimension must match rs length")
+    return cs
+
+
+def nufht_batch(nu, rs, cs, ws, tol=1e-8):
+    """Batched transform through nufht_plan_init / nufht_batch (src/_pynufht.c:144-239)."""
+    lib = L.lib()
+    rs = _vec(rs)
+    ws = _vec(ws)
+    cs = _check_batch(rs, cs)
+    cs = np.asfortranarray(cs)  # column-major, as the reference forces (src/_pynufht.c:156)
+    m, n, batch = rs.shape[0], ws.shape[0], cs.shape[1]
+    opt = L.options(tol=float(tol))
+    plan = L.NufhtPlan()
+    if lib.nufht_plan_init(ctypes.byref(plan), float(nu), L.dptr(rs), m, L.dptr(ws), n, ctypes.byref(opt)) != 0:
+        lib.nufht_plan_free(ctypes.byref(plan))
+        raise RuntimeError("nufht_plan_init failed")
+    try:
+        gs = np.empty((n, batch), dtype=np.float64, order="F")
+        ret = lib.nufht_batch(ctypes.byref(plan), L.dptr(cs), m, L.dptr(gs), n, batch, None)
+        if ret != 0:
+            raise RuntimeError("nufht_batch returned %d" % ret)
+    finally:
+        lib.nufht_plan_free(ctypes.byref(plan))
+    return np.ascontiguousarray(gs)  # C-order (n, batch) result (src/_pynufht.c:222-237)
+
+
+def nufht_batch_loop(nu, rs, cs, ws, tol=1e-8):
+    """Batch by looping single transforms over the columns (src/_pynufht.c:64-142)."""
+    rs = _vec(rs)
+    ws = _vec(ws)
+    cs = _check_batch(rs, cs)
+    out = np.empty((ws.shape[0], cs.shape[1]), dtype=np.float64)
+    for b in range(cs.shape[1]):
+        out[:, b] = nufht(nu, rs, np.ascontiguousarray(cs[:, b]), ws, tol)
+    return out

@@ -1,0 +1,567 @@
+// C ABI of libnufht_b200.so: the reference library's entry points (src/fast_hankel_nufht.h)
+// backed by the GPU executor, and this library's device-plan extension.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "executor.h"
+#include "nufht_internal.h"
+
+using hankel::DevicePlan;
+using hankel::HBox;
+using hankel::HBoxes;
+using hankel::PlanParams;
+
+struct NufhtDevicePlan {
+  std::unique_ptr<DevicePlan> dp;
+};
+
+namespace {
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int has_device() {
+  int cnt = 0;
+  if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt <= 0) {
+    cudaGetLastError();
+    return 0;
+  }
+  return 1;
+}
+
+// Host copy of a grid that may live on the device.
+int host_copy(const double* p, int len, std::vector<double>* out) {
+  out->resize((size_t)len);
+  if (is_device_ptr(p)) {
+    if (cudaMemcpy(out->data(), p, sizeof(double) * (size_t)len, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return NUFHT_E_CUDA;
+  } else {
+    std::memcpy(out->data(), p, sizeof(double) * (size_t)len);
+  }
+  return 0;
+}
+
+std::vector<HBox> to_hbox(const BoxVector& v) {
+  std::vector<HBox> out;
+  for (size_t q = 0; q < v.length; ++q) out.push_back({v.data[q].i0, v.data[q].i1, v.data[q].j0, v.data[q].j1});
+  return out;
+}
+
+BoxVector to_boxvec(const std::vector<HBox>& v) {
+  BoxVector b;
+  b.length = v.size();
+  b.capacity = v.size();
+  b.data = v.empty() ? nullptr : (Box*)std::malloc(sizeof(Box) * v.size());
+  for (size_t q = 0; q < v.size(); ++q) b.data[q] = {v[q].i0, v[q].i1, v[q].j0, v[q].j1};
+  return b;
+}
+
+// Decide which evaluation path nufht_batch takes (src/fast_hankel_nufht.c:1018-1080) and
+// fill the boxes the executor evaluates.
+void choose_path(DevicePlan* D, int min_dim_prod) {
+  long long dp = (long long)D->m * (long long)D->n;
+  D->loc_boxes.clear();
+  D->asy_boxes.clear();
+  D->dir_boxes.clear();
+  HBox whole{0, D->n - 1, 0, D->m - 1};
+  if (dp < (long long)min_dim_prod) {
+    D->path = 1;
+    D->dir_boxes.push_back(whole);
+  } else if (!hankel::is_integer(D->P.nu)) {
+    D->path = 2;
+    D->asy_boxes.push_back(whole);
+  } else {
+    D->path = 0;
+    if (D->P.K_loc >= 0) D->loc_boxes = D->plan_loc;
+    D->asy_boxes = D->plan_asy;
+    D->dir_boxes = D->plan_dir;
+  }
+}
+
+int finish_device_plan(DevicePlan* D, int device) {
+  D->device = device;
+  D->nu2 = (int)std::llround(2.0 * std::fabs(D->P.nu));
+  D->sign = (D->P.nu < 0.0 && hankel::is_odd_integer(D->P.nu)) ? -1.0 : 1.0;
+  D->build_lists();
+  return D->upload_all();
+}
+
+// ---- registry of device state for reference-style plans (NufhtPlan has no spare field)
+struct Entry {
+  const double* rs;
+  const double* ws;
+  int m, n, K_asy, K_loc;
+  double nu, tol, z_split;
+  const Box *dl, *da, *dd;
+  size_t nl, na, nd;
+  std::unique_ptr<DevicePlan> dp;
+};
+std::mutex g_reg_mu;
+std::map<const NufhtPlan*, std::unique_ptr<Entry>> g_reg;
+
+bool entry_matches(const Entry& e, const NufhtPlan* p) {
+  return e.rs == p->rs && e.ws == p->ws && e.m == p->m && e.n == p->n && e.K_asy == p->K_asy &&
+         e.K_loc == p->K_loc && e.nu == p->nu && e.tol == p->tol &&
+         (e.z_split == p->z_split || (std::isnan(e.z_split) && std::isnan(p->z_split))) &&
+         e.dl == p->boxes.loc.data && e.da == p->boxes.asy.data && e.dd == p->boxes.dir.data &&
+         e.nl == p->boxes.loc.length && e.na == p->boxes.asy.length && e.nd == p->boxes.dir.length;
+}
+
+int device_state_for(const NufhtPlan* plan, DevicePlan** out) {
+  std::lock_guard<std::mutex> lk(g_reg_mu);
+  auto it = g_reg.find(plan);
+  if (it != g_reg.end() && entry_matches(*it->second, plan)) {
+    *out = it->second->dp.get();
+    return 0;
+  }
+  if (!has_device()) return NUFHT_E_NO_DEVICE;
+  std::unique_ptr<Entry> e(new Entry);
+  e->rs = plan->rs; e->ws = plan->ws; e->m = plan->m; e->n = plan->n;
+  e->K_asy = plan->K_asy; e->K_loc = plan->K_loc; e->nu = plan->nu; e->tol = plan->tol;
+  e->z_split = plan->z_split;
+  e->dl = plan->boxes.loc.data; e->da = plan->boxes.asy.data; e->dd = plan->boxes.dir.data;
+  e->nl = plan->boxes.loc.length; e->na = plan->boxes.asy.length; e->nd = plan->boxes.dir.length;
+  std::unique_ptr<DevicePlan> D(new DevicePlan);
+  D->m = plan->m;
+  D->n = plan->n;
+  D->P.nu = plan->nu; D->P.tol = plan->tol; D->P.z_split = plan->z_split;
+  D->P.K_asy = plan->K_asy; D->P.K_loc = plan->K_loc;
+  std::memcpy(D->P.asy_coef, plan->asy_coef, sizeof(plan->asy_coef));
+  int rc;
+  if ((rc = host_copy(plan->rs, plan->m, &D->h_rs)) || (rc = host_copy(plan->ws, plan->n, &D->h_ws)))
+    return rc;
+  D->plan_loc = to_hbox(plan->boxes.loc);
+  D->plan_asy = to_hbox(plan->boxes.asy);
+  D->plan_dir = to_hbox(plan->boxes.dir);
+  choose_path(D.get(), plan->min_dim_prod);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if ((rc = finish_device_plan(D.get(), dev))) return rc;
+  e->dp = std::move(D);
+  *out = e->dp.get();
+  g_reg[plan] = std::move(e);
+  return 0;
+}
+
+void drop_device_state(const NufhtPlan* plan) {
+  std::lock_guard<std::mutex> lk(g_reg_mu);
+  g_reg.erase(plan);
+}
+
+// Run D on cs/gs that may be host or device pointers (synchronous, legacy stream).
+int run_any(DevicePlan* D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, bool zero) {
+  std::lock_guard<std::mutex> lk(D->mu);
+  if (cudaSetDevice(D->device) != cudaSuccess) return NUFHT_E_CUDA;
+  cudaStream_t st = 0;
+  const bool cdev = is_device_ptr(cs), gdev = is_device_ptr(gs);
+  const double* dc = cs;
+  double* dg = gs;
+  int ldc = ld_cs, ldg = ld_gs;
+  if (!cdev) {
+    size_t need = sizeof(double) * (size_t)D->m * (size_t)B;
+    if (need > D->stage_c_bytes) {
+      cudaFree(D->d_stage_c);
+      D->d_stage_c = nullptr;
+      D->stage_c_bytes = 0;
+      if (cudaMalloc((void**)&D->d_stage_c, need) != cudaSuccess) return NUFHT_E_CUDA;
+      D->stage_c_bytes = need;
+    }
+    if (cudaMemcpy2DAsync(D->d_stage_c, sizeof(double) * D->m, cs, sizeof(double) * (size_t)ld_cs,
+                          sizeof(double) * D->m, B, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return NUFHT_E_CUDA;
+    dc = D->d_stage_c;
+    ldc = D->m;
+  }
+  if (!gdev) {
+    size_t need = sizeof(double) * (size_t)D->n * (size_t)B;
+    if (need > D->stage_g_bytes) {
+      cudaFree(D->d_stage_g);
+      D->d_stage_g = nullptr;
+      D->stage_g_bytes = 0;
+      if (cudaMalloc((void**)&D->d_stage_g, need) != cudaSuccess) return NUFHT_E_CUDA;
+      D->stage_g_bytes = need;
+    }
+    dg = D->d_stage_g;
+    ldg = D->n;
+    if (!zero &&
+        cudaMemcpy2DAsync(dg, sizeof(double) * D->n, gs, sizeof(double) * (size_t)ld_gs,
+                          sizeof(double) * D->n, B, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return NUFHT_E_CUDA;
+  }
+  int rc = D->run(dc, ldc, dg, ldg, B, st, zero);
+  if (rc) return rc;
+  if (!gdev &&
+      cudaMemcpy2DAsync(gs, sizeof(double) * (size_t)ld_gs, dg, sizeof(double) * D->n,
+                        sizeof(double) * D->n, B, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return NUFHT_E_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return NUFHT_E_CUDA;
+  return 0;
+}
+
+// One-box evaluator for the add_* entry points.
+void run_single_box(int kind, double* gs, double nu, const double* rs, const double* cs,
+                    const double* ws, int m, int n, int K, double tol, const double* asy_coef,
+                    int batch, int ld_cs, int ld_gs, const char* who) {
+  if (!gs || !rs || !cs || !ws || m <= 0 || n <= 0 || batch <= 0) return;
+  if (!has_device()) {
+    std::fprintf(stderr, "%s: no CUDA device\n", who);
+    return;
+  }
+  std::unique_ptr<DevicePlan> D(new DevicePlan);
+  D->m = m;
+  D->n = n;
+  D->P.nu = std::fabs(nu);
+  D->P.tol = tol > 0 ? tol : 1e-8;
+  if (kind == 1) D->P.K_loc = K;
+  if (kind == 2) {
+    D->P.K_asy = K;
+    if (asy_coef) std::memcpy(D->P.asy_coef, asy_coef, sizeof(double) * 64);
+  }
+  if (host_copy(rs, m, &D->h_rs) || host_copy(ws, n, &D->h_ws)) {
+    std::fprintf(stderr, "%s: cannot read grids\n", who);
+    return;
+  }
+  HBox whole{0, n - 1, 0, m - 1};
+  if (kind == 0) D->dir_boxes.push_back(whole);
+  if (kind == 1) D->loc_boxes.push_back(whole);
+  if (kind == 2) D->asy_boxes.push_back(whole);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int rc = finish_device_plan(D.get(), dev);
+  D->sign = 1.0;
+  if (!rc) rc = run_any(D.get(), cs, ld_cs, gs, ld_gs, batch, false);
+  if (rc) std::fprintf(stderr, "%s: %s\n", who, nufht_b200_strerror(rc));
+}
+
+}  // namespace
+
+extern "C" {
+
+NufhtOptions nufht_default_options(void) {
+  NufhtOptions o;
+  o.tol = 1e-8;
+  o.max_levels = 0;
+  o.min_dim_prod = 10000;
+  o.z_split = NAN;
+  o.K_asy = 0;
+  o.K_loc = 0;
+  return o;
+}
+
+void boxes_free(Boxes* b) {
+  if (!b) return;
+  std::free(b->loc.data);
+  std::free(b->asy.data);
+  std::free(b->dir.data);
+  std::memset(b, 0, sizeof(*b));
+}
+
+Boxes generate_boxes(const double* rs, int m, const double* ws, int n, double z_split,
+                     int max_levels, int min_dim_prod, int K_loc_threshold) {
+  Boxes out;
+  std::memset(&out, 0, sizeof(out));
+  if (!rs || !ws || m <= 0 || n <= 0) return out;
+  HBoxes hb;
+  hankel::make_boxes(rs, m, ws, n, z_split, max_levels, min_dim_prod, K_loc_threshold, &hb);
+  out.loc = to_boxvec(hb.loc);
+  out.asy = to_boxvec(hb.asy);
+  out.dir = to_boxvec(hb.dir);
+  return out;
+}
+
+void split_box(const double* rs, int m, const double* ws, int n, const Box* box, double z,
+               int* ispl_out, int* jspl_out) {
+  (void)n;
+  HBox b{box->i0, box->i1, box->j0, box->j1};
+  hankel::split_box_bs(rs, m, ws, b, z, ispl_out, jspl_out);
+}
+
+int nufht_plan_init(NufhtPlan* plan, double nu, const double* rs, int m, const double* ws, int n,
+                    const NufhtOptions* opt_in) {
+  if (!plan || !rs || !ws || m <= 0 || n <= 0) return -200;
+  NufhtOptions opt = opt_in ? *opt_in : nufht_default_options();
+  drop_device_state(plan);
+  std::memset(plan, 0, sizeof(*plan));
+  plan->rs = rs;
+  plan->ws = ws;
+  plan->m = m;
+  plan->n = n;
+  plan->max_levels = opt.max_levels;
+  plan->min_dim_prod = opt.min_dim_prod;
+  PlanParams P;
+  int rc = hankel::fill_params(nu, opt, false, &P);
+  if (rc) return rc;
+  plan->nu = P.nu;
+  plan->tol = P.tol;
+  plan->z_split = P.z_split;
+  plan->K_asy = P.K_asy;
+  plan->K_loc = P.K_loc;
+  std::memcpy(plan->asy_coef, P.asy_coef, sizeof(plan->asy_coef));
+  plan->tables_loaded = 1;
+  std::vector<double> hr, hw;
+  if ((rc = host_copy(rs, m, &hr)) || (rc = host_copy(ws, n, &hw))) return rc;
+  if (hankel::check_grid(hr.data(), m)) return NUFHT_E_UNSORTED_RS;
+  if (hankel::check_grid(hw.data(), n)) return NUFHT_E_UNSORTED_WS;
+  plan->boxes = generate_boxes(hr.data(), m, hw.data(), n, P.z_split, opt.max_levels,
+                               opt.min_dim_prod, P.K_loc < 0 ? 0 : P.K_loc);
+  return 0;
+}
+
+void nufht_plan_free(NufhtPlan* plan) {
+  if (!plan) return;
+  drop_device_state(plan);
+  boxes_free(&plan->boxes);
+  std::memset(plan, 0, sizeof(*plan));
+}
+
+// Host buffers of the reference's sizes (src/fast_hankel_nufht.c:802-845).
+int nufht_scratch_init(NufhtScratch* s, const NufhtPlan* plan) {
+  if (!s || !plan) return -300;
+  std::memset(s, 0, sizeof(*s));
+  int m = plan->m, n = plan->n;
+  int Kloc = plan->K_loc < 0 ? 0 : plan->K_loc;
+  int extra = 0;
+  if (plan->K_loc >= 0) {
+    long ni = std::lround(plan->nu);
+    extra = (int)(std::labs(ni) / 2) + ((ni & 1L) ? 1 : 0);
+  }
+  s->in_buffer = (double*)std::calloc((size_t)m * 2, sizeof(double));
+  s->out_buffer = (double*)std::calloc((size_t)n * 2, sizeof(double));
+  s->real_buffer_1 = (double*)std::calloc((size_t)n, sizeof(double));
+  s->real_buffer_2 = (double*)std::calloc((size_t)n, sizeof(double));
+  s->cheb_buffer = (double*)std::calloc((size_t)Kloc + 1, sizeof(double));
+  s->bessel_buffer_1 = (double*)std::calloc((size_t)Kloc + 1, sizeof(double));
+  s->bessel_buffer_2 = (double*)std::calloc((size_t)Kloc + 1 + (size_t)extra, sizeof(double));
+  if (!s->in_buffer || !s->out_buffer || !s->real_buffer_1 || !s->real_buffer_2 ||
+      !s->cheb_buffer || !s->bessel_buffer_1 || !s->bessel_buffer_2) {
+    nufht_scratch_free(s);
+    return -301;
+  }
+  s->m_alloc = m;
+  s->n_alloc = n;
+  s->Kloc_alloc = Kloc;
+  s->extra_alloc = extra;
+  return 0;
+}
+
+void nufht_scratch_free(NufhtScratch* s) {
+  if (!s) return;
+  std::free(s->in_buffer);
+  std::free(s->out_buffer);
+  std::free(s->real_buffer_1);
+  std::free(s->real_buffer_2);
+  std::free(s->cheb_buffer);
+  std::free(s->bessel_buffer_1);
+  std::free(s->bessel_buffer_2);
+  std::memset(s, 0, sizeof(*s));
+}
+
+int nufht_batch(const NufhtPlan* plan, const double* cs, int ld_cs, double* gs, int ld_gs,
+                int batch, NufhtScratch* scratch) {
+  (void)scratch;
+  if (!plan || !cs || !gs || batch <= 0) return -400;
+  if (ld_cs < plan->m || ld_gs < plan->n) return -401;
+  DevicePlan* D = nullptr;
+  int rc = device_state_for(plan, &D);
+  if (rc) {
+    std::fprintf(stderr, "nufht_batch: %s\n", nufht_b200_strerror(rc));
+    return rc;
+  }
+  rc = run_any(D, cs, ld_cs, gs, ld_gs, batch, true);
+  if (rc) std::fprintf(stderr, "nufht_batch: %s\n", nufht_b200_strerror(rc));
+  return rc;
+}
+
+void nufht_inplace(double* gs, double nu, const double* rs, int m, const double* cs,
+                   const double* ws, int n, const NufhtOptions* opt) {
+  if (!gs || !rs || !cs || !ws || m <= 0 || n <= 0) {
+    std::fprintf(stderr, "nufht_inplace: invalid arguments\n");
+    return;
+  }
+  NufhtPlan plan;
+  std::memset(&plan, 0, sizeof(plan));
+  if (nufht_plan_init(&plan, nu, rs, m, ws, n, opt) != 0) {
+    std::fprintf(stderr, "nufht_inplace: plan init failed\n");
+    nufht_plan_free(&plan);
+    return;
+  }
+  if (nufht_batch(&plan, cs, m, gs, n, 1, nullptr) != 0)
+    std::fprintf(stderr, "nufht_inplace: batch execution failed\n");
+  nufht_plan_free(&plan);
+}
+
+double* nufht(double nu, const double* rs, int m, const double* cs, const double* ws, int n,
+              const NufhtOptions* opt) {
+  double* gs = (double*)std::calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+  if (!gs) return nullptr;
+  nufht_inplace(gs, nu, rs, m, cs, ws, n, opt);
+  return gs;
+}
+
+void add_dir(double* gs, double nu, const double* rs, const double* cs, const double* ws, int m,
+             int n) {
+  run_single_box(0, gs, nu, rs, cs, ws, m, n, 0, 1e-8, nullptr, 1, m, n, "add_dir");
+}
+
+void add_dir_batch(double* gs, double nu, const double* rs, const double* cs, const double* ws,
+                   int m, int n, int batch, int ld_cs, int ld_gs) {
+  run_single_box(0, gs, nu, rs, cs, ws, m, n, 0, 1e-8, nullptr, batch, ld_cs, ld_gs, "add_dir_batch");
+}
+
+void add_loc(double* gs, double nu, const double* rs, const double* cs, const double* ws, int m,
+             int n, int K, double*, double*, double*) {
+  if (!hankel::is_integer(nu)) {
+    std::fprintf(stderr, "add_loc: nu must be integer\n");
+    return;
+  }
+  run_single_box(1, gs, nu, rs, cs, ws, m, n, K, 1e-8, nullptr, 1, m, n, "add_loc");
+}
+
+void add_loc_batch(double* gs, double nu, const double* rs, const double* cs, const double* ws,
+                   int m, int n, int K, int batch, int ld_cs, int ld_gs, double*, double*, double*) {
+  if (!hankel::is_integer(nu)) {
+    std::fprintf(stderr, "add_loc_batch: nu must be integer\n");
+    return;
+  }
+  run_single_box(1, gs, nu, rs, cs, ws, m, n, K, 1e-8, nullptr, batch, ld_cs, ld_gs, "add_loc_batch");
+}
+
+void add_asy(double* gs, double nu, const double* rs, const double* cs, const double* ws, int m,
+             int n, int K, double tol, const double* asy_coef, double*, double*, double*, double*) {
+  run_single_box(2, gs, nu, rs, cs, ws, m, n, K, tol, asy_coef, 1, m, n, "add_asy");
+}
+
+void add_asy_batch(double* gs, double nu, const double* rs, const double* cs, const double* ws,
+                   int m, int n, int K, double tol, const double* asy_coef, int batch, int ld_cs,
+                   int ld_gs, double*, double*) {
+  run_single_box(2, gs, nu, rs, cs, ws, m, n, K, tol, asy_coef, batch, ld_cs, ld_gs, "add_asy_batch");
+}
+
+// ------------------------------- extension -------------------------------
+
+int nufht_b200_plan_create(NufhtDevicePlan** out, double nu, const double* rs, int m,
+                           const double* ws, int n, const NufhtOptions* opt_in, int flags,
+                           int device) {
+  if (!out) return -200;
+  *out = nullptr;
+  if (!rs || !ws || m <= 0 || n <= 0) return -200;
+  if (flags & ~(NUFHT_B200_MIXED | NUFHT_B200_EXTENDED_TABLES)) return NUFHT_E_BAD_FLAGS;
+  NufhtOptions opt = opt_in ? *opt_in : nufht_default_options();
+  std::unique_ptr<DevicePlan> D(new DevicePlan);
+  int rc = hankel::fill_params(nu, opt, (flags & NUFHT_B200_EXTENDED_TABLES) != 0, &D->P);
+  if (rc) return rc;
+  if (!has_device()) return NUFHT_E_NO_DEVICE;
+  if (cudaSetDevice(device) != cudaSuccess) return NUFHT_E_CUDA;
+  D->m = m;
+  D->n = n;
+  D->flags = flags;
+  if ((rc = host_copy(rs, m, &D->h_rs)) || (rc = host_copy(ws, n, &D->h_ws))) return rc;
+  if (hankel::check_grid(D->h_rs.data(), m)) return NUFHT_E_UNSORTED_RS;
+  if (hankel::check_grid(D->h_ws.data(), n)) return NUFHT_E_UNSORTED_WS;
+  HBoxes hb;
+  hankel::make_boxes(D->h_rs.data(), m, D->h_ws.data(), n, D->P.z_split, opt.max_levels,
+                    opt.min_dim_prod, D->P.K_loc < 0 ? 0 : D->P.K_loc, &hb);
+  D->plan_loc = hb.loc;
+  D->plan_asy = hb.asy;
+  D->plan_dir = hb.dir;
+  choose_path(D.get(), opt.min_dim_prod);
+  if ((rc = finish_device_plan(D.get(), device))) return rc;
+  NufhtDevicePlan* h = new NufhtDevicePlan;
+  h->dp = std::move(D);
+  *out = h;
+  return 0;
+}
+
+int nufht_b200_execute(NufhtDevicePlan* plan, const double* cs, int ld_cs, double* gs, int ld_gs,
+                       int batch, void* stream) {
+  if (!plan || !cs || !gs || batch <= 0) return -400;
+  DevicePlan* D = plan->dp.get();
+  if (ld_cs < D->m || ld_gs < D->n) return -401;
+  std::lock_guard<std::mutex> lk(D->mu);
+  return D->run(cs, ld_cs, gs, ld_gs, batch, (cudaStream_t)stream, true);
+}
+
+int nufht_b200_plan_info(const NufhtDevicePlan* plan, NufhtB200Info* info) {
+  if (!plan || !info) return -400;
+  const DevicePlan* D = plan->dp.get();
+  std::memset(info, 0, sizeof(*info));
+  info->nu = D->P.nu;
+  info->tol = D->P.tol;
+  info->z_split = D->P.z_split;
+  info->K_asy = D->P.K_asy;
+  info->K_loc = D->P.K_loc;
+  info->n_loc = (long)D->loc_boxes.size();
+  info->n_asy = (long)D->asy_boxes.size();
+  info->n_dir = (long)D->dir_boxes.size();
+  info->fft_points = D->total_cells;
+  info->spread_width = D->W;
+  info->path = D->path;
+  info->workspace_bytes = D->ws_bytes;
+  return 0;
+}
+
+void nufht_b200_plan_destroy(NufhtDevicePlan* plan) { delete plan; }
+
+long nufht_b200_plan_boxes(const NufhtDevicePlan* plan, int* out, long cap) {
+  if (!plan) return -400;
+  const DevicePlan* D = plan->dp.get();
+  long tot = (long)(D->plan_loc.size() + D->plan_asy.size() + D->plan_dir.size());
+  if (out && cap >= tot) {
+    long p = 0;
+    for (const auto* v : {&D->plan_loc, &D->plan_asy, &D->plan_dir})
+      for (const HBox& b : *v) {
+        out[4 * p] = b.i0; out[4 * p + 1] = b.i1; out[4 * p + 2] = b.j0; out[4 * p + 3] = b.j1;
+        ++p;
+      }
+  }
+  return tot;
+}
+
+const char* nufht_b200_strerror(int code) {
+  switch (code) {
+    case 0: return "success";
+    case -1: return "tolerance below 1e-15";
+    case -2: return "only integer |nu| <= 200 and half-integer |nu| <= 19/2 are implemented";
+    case -3: case -4: case -5: case -6: return "table index out of range";
+    case -100: return "NULL plan or options";
+    case -200: return "NULL grid or non-positive size";
+    case -300: return "NULL scratch or plan";
+    case -301: return "scratch allocation failed";
+    case -400: return "invalid argument";
+    case -401: return "leading dimension smaller than the grid size";
+    case -402: case -403: return "allocation failed";
+    case NUFHT_E_UNSORTED_RS: return "rs must be finite, non-negative and non-decreasing";
+    case NUFHT_E_UNSORTED_WS: return "ws must be finite, non-negative and non-decreasing";
+    case NUFHT_E_CUDA: return "CUDA runtime or cuFFT error";
+    case NUFHT_E_NO_DEVICE: return "no CUDA device";
+    case NUFHT_E_TOO_LARGE: return "sizes exceed what this entry point accepts";
+    case NUFHT_E_BAD_FLAGS: return "unknown flag bits";
+    default: return "unknown error";
+  }
+}
+
+long long nufht_b200_launch_count(void) { return hankel::g_launch_counter.load(); }
+
+int nufht_b200_besselj(double nu, const double* x, double* out, long count, void* stream) {
+  if (!x || !out || count < 0) return -400;
+  return hankel::run_besselj(nu, x, out, count, (cudaStream_t)stream);
+}
+
+const char* nufht_b200_table_source(void) { return hankel::tables_source(); }
+
+}  // extern "C"
