@@ -213,6 +213,14 @@ long long nufht_b200_launch_count(void);
  * device special-function code. */
 int nufht_b200_besselj(double nu, const double *x, double *out, long count, void *stream);
 
+/* Device timing of the phases of every transform executed while enabled: CUDA events on
+ * the launching stream.  nufht_b200_phase_times() waits for them, adds the milliseconds
+ * per phase into ms[0..nphase) -- 0 zeroing of g, 1 local projection, 2 local evaluation,
+ * 3 asymptotic spreading, 4 FFT, 5 asymptotic interpolation, 6 direct boxes -- releases
+ * them and returns how many phase records it read. */
+void nufht_b200_set_phase_timing(int on);
+int nufht_b200_phase_times(double *ms, int nphase);
+
 /* Where the planning tables were read from (a cache file path), or "generated". */
 const char *nufht_b200_table_source(void);
 

@@ -109,6 +109,8 @@ def _declare(lib):
         "nufht_b200_besselj": (ctypes.c_int, [ctypes.c_double, vp, vp, ctypes.c_long, vp]),
         "nufht_b200_table_source": (ctypes.c_char_p, []),
         "nufht_b200_write_tables": (ctypes.c_int, [ctypes.c_char_p]),
+        "nufht_b200_set_phase_timing": (None, [ctypes.c_int]),
+        "nufht_b200_phase_times": (ctypes.c_int, [c_double_p, ctypes.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -126,6 +128,16 @@ def lib():
                                "(there is no CPU fallback)")
         _lib = _declare(ctypes.CDLL(LIB_PATH))
     return _lib
+
+
+PHASES = ("zero", "loc_proj", "loc_eval", "asy_spread", "asy_fft", "asy_interp", "dir")
+
+
+def phase_times():
+    """Milliseconds per phase accumulated since timing was enabled (then reset)."""
+    ms = np.zeros(len(PHASES))
+    lib().nufht_b200_phase_times(ms.ctypes.data_as(c_double_p), len(PHASES))
+    return dict(zip(PHASES, ms.tolist()))
 
 
 def strerror(code):

@@ -564,4 +564,11 @@ int nufht_b200_besselj(double nu, const double* x, double* out, long count, void
 
 const char* nufht_b200_table_source(void) { return hankel::tables_source(); }
 
+void nufht_b200_set_phase_timing(int on) { hankel::g_phase_timing.store(on != 0); }
+
+int nufht_b200_phase_times(double* ms, int nphase) {
+  if (!ms || nphase <= 0) return -400;
+  return hankel::phase_times(ms, nphase);
+}
+
 }  // extern "C"

@@ -5,7 +5,6 @@
 #include <cufft.h>
 
 #include <atomic>
-#include <map>
 #include <mutex>
 #include <vector>
 
@@ -23,24 +22,40 @@ struct LocBoxD {
 };
 struct ProjItem { int box, j0, nj; };
 struct EvalItem { int box, i0, ni; };
-struct DirItem { int i0, ni, j0, nj; };
+// Direct work item: targets [i0, i0+ni), sources [j0, j0+nj); `lanes` threads share one
+// target (thin boxes) and split its sources.
+struct DirItem { int i0, ni, j0, nj, lanes; };
 
 // Geometry of one asymptotic box's type-3 transform: sources x = r - C, targets s = k - D,
-// spreading grid spacing h (cells l in [-half, half]), FFT length n2, and the offset of its
-// grid (in cells per vector) in the workspace.
+// spreading grid spacing h (cells l in [-half, half]), FFT length n2, its rows in the
+// per-cell deconvolution and per-target phase tables, and its place in the workspace.
+// The workspace holds, per FFT group of boxes with equal n2, the cells of all its boxes
+// and all V = NLP * B vectors interleaved: element (cell q, vector v) of the box sits at
+// (row0 + q * rstride) * V + v, so neighbouring vectors are neighbouring addresses and
+// cuFFT sees nbox * V transforms with stride nbox * V and distance 1.
 struct AsyBoxD {
   int i0, i1, j0, j1;
   double C, D, h;
   int half, n2;
-  long long cell_off;
+  int mode;             // 0: CTAs own grid tiles; 1: CTAs own source chunks (dense boxes)
+  int cls;              // kernel class (oversampling and kernel width)
+  long long row0;       // first grid row of this box
+  int rstride;          // grid rows between consecutive cells of this box
+  long long corr_off;   // first of 2 half + 1 entries in the cell table
+  long long post_off;   // first of i1 - i0 + 1 entries in the target table
 };
+// Spreading work item.  mode 0: cells [l_start, l_start+ncell) of the box, FFT index
+// fft_start.., sources [js, je) whose support meets them; mode 1: all taps of sources
+// [js, je) into a window of cells [l_start, l_start+ncell) added atomically; mode 2: FFT
+// indices [fft_start, fft_start+ncell) of the zero padding.
 struct SpreadItem {
-  int box, l_start, fft_start, ncell, js, je, padding;
+  int box, mode, l_start, fft_start, ncell, js, je;
 };
 struct InterpItem { int box, ks, ke; };
 struct FftGroup {
-  int n2, box0, nbox;
-  long long cell_off;
+  int n2, nbox, mode;
+  long long row0;  // first grid row; the group spans n2 * nbox rows
+  cufftHandle plan;
 };
 
 struct AsyConst {
@@ -53,7 +68,17 @@ struct AsyConst {
   double qwpsi[kMaxQuad];   // weight * psi(node)
 };
 
+// A kernel class: oversampling factor sigma of both type-3 stages, kernel width W and
+// shape beta, and the contiguous ranges of its boxes' spreading / interpolation items.
+struct AsyClass {
+  double sigma;
+  int W;
+  AsyConst ac;
+  int spread0, nspread, interp0, ninterp;
+};
+
 int spread_width_for_tol(double tol);
+int spread_width(double tol, double sigma);
 
 struct DevicePlan {
   int device = 0;
@@ -77,8 +102,12 @@ struct DevicePlan {
   std::vector<SpreadItem> spread;
   std::vector<InterpItem> interp;
   std::vector<FftGroup> groups;
-  long long total_cells = 0;
-  AsyConst ac{};
+  std::vector<AsyClass> classes;
+  long long total_cells = 0;       // grid rows: sum of n2 over asymptotic boxes
+  long long chunk_cell_begin = 0;  // grid rows of the mode-1 boxes (zeroed before spreading)
+  long long chunk_cell_end = 0;
+  long long total_corr = 0, total_post = 0;
+  int NLP = 0;                     // 2 (K_asy + 1)
 
   // device copies
   double *d_rs = nullptr, *d_ws = nullptr;
@@ -89,15 +118,18 @@ struct DevicePlan {
   AsyBoxD* d_asyb = nullptr;
   SpreadItem* d_spread = nullptr;
   InterpItem* d_interp = nullptr;
+  double* d_corr = nullptr;   // 1 / psi-hat of the second stage, per box cell
+  double2* d_post = nullptr;  // exp(i (phi + k C)) / psi-hat(theta_k), per box target
 
   // workspace, sized for the largest batch executed so far
   int ws_B = 0;
+  int fft_B = 0;             // batch size the FFT plans were made for
+  size_t fft_work_bytes = 0;
   size_t ws_bytes = 0;
   double2* d_grid = nullptr;
   double* d_partial = nullptr;
   double* d_cheb = nullptr;
   void* d_fft_work = nullptr;
-  std::map<int, cufftHandle> fft_plans;
 
   // staging for host-pointer calls through the reference-compatible entry points
   double* d_stage_c = nullptr;
@@ -110,12 +142,20 @@ struct DevicePlan {
   void build_lists();
   int upload_all();
   int ensure_workspace(int B);
+  int ensure_fft(int B);
+  void release_fft();
   // g (+)= H c on stream st; cs / gs are device pointers.
   int run(const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
           bool zero_output);
 };
 
 extern std::atomic<long long> g_launch_counter;
+extern std::atomic<bool> g_phase_timing;
+
+// Phases of run() reported by the optional device timers.
+enum { kPhaseZero = 0, kPhaseLocProj, kPhaseLocEval, kPhaseSpread, kPhaseFft, kPhaseInterp, kPhaseDir,
+       kNumPhases };
+int phase_times(double* ms, int nphase);
 
 int run_besselj(double nu, const double* x, double* out, long count, cudaStream_t st);
 

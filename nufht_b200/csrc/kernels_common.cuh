@@ -1,0 +1,45 @@
+// Helpers shared by the executor's kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#include "executor.h"
+
+namespace hankel {
+
+#define NUFHT_CUDA_TRY(expr)                                                               \
+  do {                                                                                     \
+    cudaError_t _e = (expr);                                                               \
+    if (_e != cudaSuccess) {                                                               \
+      std::fprintf(stderr, "nufht_b200: %s failed: %s\n", #expr, cudaGetErrorString(_e));  \
+      return NUFHT_E_CUDA;                                                                 \
+    }                                                                                      \
+  } while (0)
+
+#define NUFHT_LAUNCH_CHECK()                                                               \
+  do {                                                                                     \
+    g_launch_counter.fetch_add(1, std::memory_order_relaxed);                              \
+    cudaError_t _e = cudaGetLastError();                                                   \
+    if (_e != cudaSuccess) {                                                               \
+      std::fprintf(stderr, "nufht_b200: kernel launch failed: %s\n", cudaGetErrorString(_e)); \
+      return NUFHT_E_CUDA;                                                                 \
+    }                                                                                      \
+  } while (0)
+
+// Exponential-of-semicircle kernel in grid units, support |u| < W/2.
+__device__ __forceinline__ double es_kernel(double u, double inv_half_w, double beta) {
+  double z = u * inv_half_w;
+  double s = 1.0 - z * z;
+  return s > 0.0 ? exp(beta * (sqrt(s) - 1.0)) : 0.0;
+}
+
+// Fourier transform of the kernel, int psi(u) cos(om u) du, by Gauss-Legendre quadrature.
+__device__ __forceinline__ double es_hat(const AsyConst& P, double om) {
+  double s = 0.0;
+  for (int q = 0; q < P.nq; ++q) s += P.qwpsi[q] * cos(om * P.qx[q]);
+  return 2.0 * s;
+}
+
+}  // namespace hankel

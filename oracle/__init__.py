@@ -36,9 +36,8 @@ def _p(a):
 def lib():
     global _o
     if _o is None:
-        if not os.path.exists(LIB_PATH):
-            from . import build as _b
-            _b.build()
+        from . import build as _b
+        _b.build()  # rebuilds only when the sources are newer than the library
         o = ctypes.CDLL(LIB_PATH)
         o.oracle_load_tables.argtypes = [ctypes.c_char_p]
         o.oracle_plan_params.argtypes = [cd, cd, cd, ci, ci, vp, vp, vp, vp]

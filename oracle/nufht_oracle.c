@@ -601,7 +601,9 @@ void oracle_add_loc_batch(double *gs, double nu, const double *rs, const double 
 #pragma omp parallel for schedule(static) num_threads(g_threads)
     for (int l = 0; l <= K; ++l) {
         for (int k = 0; k < m; ++k) {
-            double v = o_cheb_val(nu_int, l, rs[k] / r_end);
+            /* r_end = 0 (all sources at the origin): the reference divides by zero and
+             * returns NaN; only the l = 0 term survives there, so any x serves. */
+            double v = o_cheb_val(nu_int, l, r_end > 0.0 ? rs[k] / r_end : 0.0);
             for (int t = 0; t < batch; ++t) cheb[(size_t)t * stride + l] += v * cs[(size_t)t * ld_cs + k];
         }
     }
