@@ -1,0 +1,388 @@
+"""Benchmark of the batched NUFHT on B200: forward H c plus adjoint H^T y.
+
+Metric (the reference's headline): Gpts*cols/s = 2 (N + M) B / (t_fwd + t_adj).
+Workload: nu = 0; N = M = 1e6 sources r and targets k drawn as 1000 (1 - U[0,1)) and sorted;
+B = 32 columns of c ~ N(0,1) (seed 1, plus the rank); tol 1e-8.  One step = one forward
+transform on (r -> k) and one adjoint transform on (k -> r) of B columns each.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--precision fp64|mixed]
+
+Under torchrun each rank transforms its own B columns with the same grids (weak scaling,
+no data-path collective); the reported time is the maximum over ranks.  Rank 0 prints one
+JSON line.  --impl reference times the reference's CPU path (its own planner and driver,
+compiled from its sources into oracle/_ref, over the oracle's evaluators) on the host cores.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gpts*cols/s fwd+adjoint at tol 1e-8, mixed vs plain FP64 GPU, vs host CPU"
+UNIT = "Gpts*cols/s"
+
+
+def make_inputs(N, M, B, seed):
+    rng = np.random.default_rng(1)
+    r = np.sort(1000.0 * (1.0 - rng.random(N)))
+    k = np.sort(1000.0 * (1.0 - rng.random(M)))
+    crng = np.random.default_rng(1 + seed)
+    c = crng.standard_normal((B, N))  # column t = row t (column-major N x B)
+    y = crng.standard_normal((B, M))
+    return r, k, c, y
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[4:8]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_from_profiles(kernel):
+    """DRAM bytes per launch of `kernel` at this workload from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic_cfg2.json")) as f:
+            t = json.load(f)
+        return t.get(kernel)
+    except Exception:
+        return None
+
+
+class StdoutToStderr:
+    """Route C-level writes to stdout (the reference prints when it loads its tables) to
+    stderr, so that stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *a):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def run_cpu_reference(N, M, B_sample, steps, warmup, threads):
+    """The reference's CPU path: oracle/_ref (the reference's own planner and nufht_batch,
+    compiled from its sources, over the oracle's evaluators with the type-3 NUFFT), or the
+    oracle's restatement of the driver when oracle/_ref is absent.  Planning (once per
+    direction) is outside the timed region, as the reference's benchmark notebook times
+    nufht_batch.  Returns (seconds per fwd+adj step, kind)."""
+    import oracle
+    oracle.set_threads(threads)
+    r, k, c, y = make_inputs(N, M, B_sample, 0)
+    cF = np.asfortranarray(c.T)
+    yF = np.asfortranarray(y.T)
+    kind = "reference" if oracle.ref_available() else "port"
+    if kind == "reference":
+        from nufht_b200 import _lib as L
+        R = oracle.ref()
+        R.oracle_set_type3_mode(oracle.T3_NUFFT)
+        R.oracle_set_threads(threads)
+        plans = []
+        for (a, b) in ((r, k), (k, r)):
+            p = L.NufhtPlan()
+            opt = R.nufht_default_options()
+            opt.tol = 1e-8
+            rc = R.nufht_plan_init(ctypes.byref(p), 0.0, a.ctypes.data_as(ctypes.c_void_p), len(a),
+                                   b.ctypes.data_as(ctypes.c_void_p), len(b), ctypes.byref(opt))
+            assert rc == 0, rc
+            plans.append(p)
+        gF = np.zeros((M, B_sample), order="F")
+        hF = np.zeros((N, B_sample), order="F")
+
+        def step():
+            R.nufht_batch(ctypes.byref(plans[0]), cF.ctypes.data_as(ctypes.c_void_p), N,
+                          gF.ctypes.data_as(ctypes.c_void_p), M, B_sample, None)
+            R.nufht_batch(ctypes.byref(plans[1]), yF.ctypes.data_as(ctypes.c_void_p), M,
+                          hF.ctypes.data_as(ctypes.c_void_p), N, B_sample, None)
+    else:
+        def step():
+            oracle.nufht_batch(0.0, r, k, cF, 1e-8, mode=oracle.T3_NUFFT)
+            oracle.nufht_batch(0.0, k, r, yF, 1e-8, mode=oracle.T3_NUFFT)
+    for _ in range(warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    dt = (time.perf_counter() - t0) / steps
+    return dt, kind
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--n", type=int, default=1000000)
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    N = M = args.n
+    B = args.batch
+    tol = 1e-8
+    workload = "nu=0, N=M=%d uniform on (0,1000], batch %d, tol 1e-8, forward + adjoint" % (N, B)
+    config = {"workload": workload, "nu": 0, "N": N, "M": M, "batch_per_gpu": B, "tol": tol,
+              "global_batch": B * world, "precision": args.precision,
+              "parallelism": "dp%d (independent column blocks per GPU, no collective)" % world,
+              "l2": "inputs larger than L2 (c and y 256 MB each, FFT workspace > 1 GB)"}
+    cores = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        B_s = max(1, min(B, cores))
+        with StdoutToStderr():
+            dt, kind = run_cpu_reference(N, M, B_s, max(1, min(args.steps, 2)), 0 if args.warmup <= 0 else 1, cores)
+        value = 2.0 * (N + M) * B_s / dt / 1e9
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+                "steps": max(1, min(args.steps, 2)), "warmup": 1, "ms_per_step": dt * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded numpy draws with the workload's shapes)", "config": config,
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                                 "sample": "%d of %d columns of the workload, fwd+adj, type-3 by the oracle's "
+                                           "NUFFT (eps = tol); planning excluded" % (B_s, B)},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=dev)
+        pg = True
+    from nufht_b200 import DevicePlan
+    from nufht_b200 import _lib as L
+    lib = L.lib()
+    mixed = args.precision == "mixed"
+    r, k, c_h, y_h = make_inputs(N, M, B, rank)
+    pf = DevicePlan(0.0, r, k, tol, mixed=mixed, device=local)
+    pa = DevicePlan(0.0, k, r, tol, mixed=mixed, device=local)
+    c = torch.tensor(c_h, device=dev)
+    y = torch.tensor(y_h, device=dev)
+    g = torch.empty((B, M), dtype=torch.float64, device=dev)
+    h = torch.empty((B, N), dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream(dev)
+
+    def step():
+        pf.execute_columns(c, g, st)
+        pa.execute_columns(y, h, st)
+
+    def barrier():
+        if pg:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    barrier()
+    launches0 = lib.nufht_b200_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(st)
+        for _ in range(args.steps):
+            step()
+        e1.record(st)
+        barrier()
+    launches = lib.nufht_b200_launch_count() - launches0
+    ms = e0.elapsed_time(e1) / args.steps
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = 2.0 * (N + M) * B * world / (ms * 1e-3) / 1e9
+
+    # Per-kernel device times over a second run of the same steps (CUDA events on the
+    # launching stream around each phase), for the roofline of the dominant kernel.
+    lib.nufht_b200_set_phase_timing(1)
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize(dev)
+    lib.nufht_b200_set_phase_timing(0)
+    phases = {kk: v / args.steps for kk, v in L.phase_times().items()}
+
+    # End to end through the reference-facing C ABI: nufht_plan_init / nufht_batch with host
+    # buffers (pinned), the copies inside the timed region.
+    plans = []
+    for (a, b) in ((r, k), (k, r)):
+        p = L.NufhtPlan()
+        opt = L.options(tol=tol)
+        assert lib.nufht_plan_init(ctypes.byref(p), 0.0, L.dptr(a), len(a), L.dptr(b), len(b), ctypes.byref(opt)) == 0
+        plans.append(p)
+    cp = torch.tensor(c_h).pin_memory()
+    yp = torch.tensor(y_h).pin_memory()
+    gp = torch.empty((B, M), dtype=torch.float64).pin_memory()
+    hp = torch.empty((B, N), dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        rc1 = lib.nufht_batch(ctypes.byref(plans[0]), ctypes.c_void_p(cp.data_ptr()), N,
+                              ctypes.c_void_p(gp.data_ptr()), M, B, None)
+        rc2 = lib.nufht_batch(ctypes.byref(plans[1]), ctypes.c_void_p(yp.data_ptr()), M,
+                              ctypes.c_void_p(hp.data_ptr()), N, B, None)
+        assert rc1 == 0 and rc2 == 0
+
+    for _ in range(2):
+        e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if pg:
+        t = torch.tensor([e2e_s], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    for p in plans:
+        lib.nufht_plan_free(ctypes.byref(p))
+    e2e = {"value": 2.0 * (N + M) * B * world / e2e_s / 1e9, "unit": UNIT,
+           "h2d_bytes_per_step": 8 * (N * B + M * B), "d2h_bytes_per_step": 8 * (M * B + N * B),
+           "api": "nufht_plan_init + nufht_batch (C ABI) on pinned host buffers"}
+
+    # Roofline of the dominant kernel (the phase with the largest device time).
+    hbm, hbm_kind = peaks()
+    sf = np.zeros(12)
+    sa = np.zeros(12)
+    lib.nufht_b200_plan_stats(pf._h, sf.ctypes.data_as(L.c_double_p), 12)
+    lib.nufht_b200_plan_stats(pa._h, sa.ctypes.data_as(L.c_double_p), 12)
+    V = sf[10] * B
+    byts = {  # algorithmic bytes per fwd+adj step (both plans), FP64 storage
+        "asy_spread": sum(8.0 * s[0] * (B + 1) + 16.0 * s[2] * V for s in (sf, sa)),
+        "asy_fft": sum(2 * 16.0 * s[2] * V for s in (sf, sa)),
+        "asy_interp": sum(16.0 * s[8] * V + 8.0 * s[1] * (2 * B + 1) for s in (sf, sa)),
+    }
+    flops = {
+        "asy_spread": sum(4.0 * s[3] * V for s in (sf, sa)),
+        "asy_interp": sum(4.0 * s[4] * V for s in (sf, sa)),
+        "dir": sum(2.0 * s[5] * B for s in (sf, sa)),
+    }
+    dom = max(phases, key=lambda kk: phases[kk])
+    kname = {"asy_spread": "k_asy_spread", "asy_interp": "k_asy_interp", "asy_fft": "cufft",
+             "dir": "k_dir", "loc_proj": "k_loc_proj", "loc_eval": "k_loc_eval", "zero": "memset"}[dom]
+    fp64 = ctypes.c_double(0.0)
+    lib.nufht_b200_fp64_peak(ctypes.byref(fp64))
+    t_dom = phases[dom] * 1e-3  # per step (2 launches: forward and adjoint plan)
+    ach_gbs = byts.get(dom, 0.0) / t_dom / 1e9 if t_dom > 0 else 0.0
+    roofline = {"kernel": kname, "bound": "hbm", "achieved": ach_gbs, "peak": hbm, "unit": "GB/s",
+                "frac": ach_gbs / hbm, "peak_source": hbm_kind + " (MEASURED_PEAKS.json hbm_gbs)"
+                if hbm_kind == "measured" else "fallback",
+                "traffic": traffic_from_profiles(kname),
+                "algorithmic_bytes_per_launch": byts.get(dom, 0.0) / 2,
+                "avg_launch_ms": phases[dom] / 2}
+    if dom in flops:
+        ach_tf = flops[dom] / t_dom / 1e12
+        roofline["fp64"] = {"achieved": ach_tf, "peak": fp64.value, "unit": "TFLOP/s",
+                            "frac": ach_tf / fp64.value if fp64.value > 0 else None,
+                            "peak_source": "measured FP64 FMA probe (nufht_b200_fp64_peak)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        B_s = max(1, min(B, cores))
+        with StdoutToStderr():
+            dt, kind = run_cpu_reference(N, M, B_s, 1, 0, cores)
+        cpu = {"value": 2.0 * (N + M) * B_s / dt / 1e9, "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": "%d of %d columns, fwd+adj, planning excluded, type-3 by the oracle's NUFFT" % (B_s, B)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if not mixed else "f32/f64",
+                "data": "synthetic (seeded numpy draws with the workload's shapes)", "config": config,
+                "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches),
+                "phases_ms_per_step": phases, "roofline": roofline, "cpu_baseline": cpu,
+                "plan": pf.info()}
+        print(json.dumps(line))
+    pf.close()
+    pa.close()
+    if pg:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

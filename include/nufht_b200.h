@@ -221,6 +221,15 @@ int nufht_b200_besselj(double nu, const double *x, double *out, long count, void
 void nufht_b200_set_phase_timing(int on);
 int nufht_b200_phase_times(double *ms, int nphase);
 
+/* Algorithmic work of a plan, per batch column where it scales with the batch:
+ * out[0..11] = asymptotic sources, asymptotic targets, FFT cells, spreading taps,
+ * interpolation taps, direct pairs, local sources, local targets, FFT cells read by
+ * interpolation, FFT flops per vector, expansion terms (2 (K_asy + 1)), K_loc + 1. */
+int nufht_b200_plan_stats(const NufhtDevicePlan *plan, double *out, int n);
+
+/* Measured FP64 fused-multiply-add throughput of the current device (TFLOP/s). */
+int nufht_b200_fp64_peak(double *tflops);
+
 /* Where the planning tables were read from (a cache file path), or "generated". */
 const char *nufht_b200_table_source(void);
 

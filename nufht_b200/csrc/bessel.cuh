@@ -5,7 +5,8 @@
 //   bessel_j_orders(...) J_0(z) .. J_nmax(z) at one argument (Miller's algorithm)
 //
 // Methods (absolute error target ~1e-15, checked against mpmath values):
-//   * x >= 17: J_0 and J_1 from Hankel's expansion (bessel_j01_large), then the upward
+//   * J_0 and J_1: Hankel's expansion for x >= 17 (bessel_j01_large), piecewise Chebyshev
+//     expansions for x < 17 (bessel_j01_small); higher orders with x > n by the upward
 //     recurrence J_{k+1} = (2k/x) J_k - J_{k-1}, stable while k < x;
 //   * x <= 2 sqrt(n+1): power series  J_n(x) = sum_k (-x^2/4)^k (x/2)^n / (k! (n+k)!),
 //     whose terms decrease from the first one in this range (no cancellation);
@@ -18,6 +19,8 @@
 
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include "bessel_j01_table.h"
 
 namespace hankel {
 
@@ -66,23 +69,48 @@ __device__ inline void bessel_j01_large(double x, double* J0, double* J1) {
 
 constexpr double kHankelMinX = 17.0;
 
-__device__ inline double bessel_jn(int n, double x) {
-  if (x >= kHankelMinX) {
-    double a, b;
-    bessel_j01_large(x, &a, &b);
-    if (n == 0) return a;
-    if (n == 1) return b;
-    if (x > (double)n) {
-      double tox = 2.0 / x;
-      for (int k = 1; k < n; ++k) {
-        double c = (double)k * tox * b - a;
-        a = b;
-        b = c;
-      }
-      return b;
-    }
+// J_0(x) and J_1(x) for 0 <= x < 17 from the piecewise Chebyshev expansions of
+// bessel_j01_table.h (unit intervals, Clenshaw summation; error below 2e-16).
+__device__ inline void bessel_j01_small(double x, double* J0, double* J1) {
+  int a = (int)x;
+  a = a < 0 ? 0 : (a > kJ01Intervals - 1 ? kJ01Intervals - 1 : a);
+  const double t = 2.0 * (x - (double)a) - 1.0, t2 = 2.0 * t;
+  const double* c0 = kJ01Cheb[0][a];
+  const double* c1 = kJ01Cheb[1][a];
+  double b1 = 0.0, b2 = 0.0, d1 = 0.0, d2 = 0.0;
+#pragma unroll
+  for (int k = kJ01Coefs - 1; k > 0; --k) {
+    double bn = fma(t2, b1, c0[k] - b2);
+    double dn = fma(t2, d1, c1[k] - d2);
+    b2 = b1;
+    b1 = bn;
+    d2 = d1;
+    d1 = dn;
   }
-  if (x == 0.0) return n == 0 ? 1.0 : 0.0;
+  *J0 = fma(t, b1, c0[0] - b2);
+  *J1 = fma(t, d1, c1[0] - d2);
+}
+
+__device__ inline double bessel_jn(int n, double x) {
+  double a, b;
+  if (x >= kHankelMinX) {
+    bessel_j01_large(x, &a, &b);
+  } else if (n <= 1 || x > (double)n) {
+    bessel_j01_small(x, &a, &b);
+  }
+  if (n == 0) return a;
+  if (n == 1) return b;
+  if (x > (double)n && (x >= kHankelMinX || x > 2.0 * sqrt((double)n + 1.0))) {
+    // upward recurrence, stable while k < x
+    const double tox = 2.0 / x;
+    for (int k = 1; k < n; ++k) {
+      double c = (double)k * tox * b - a;
+      a = b;
+      b = c;
+    }
+    return b;
+  }
+  if (x == 0.0) return 0.0;
   if (x <= 2.0 * sqrt((double)n + 1.0)) {
     double h = 0.5 * x, t = 1.0;
     for (int i = 1; i <= n; ++i) t *= h / (double)i;

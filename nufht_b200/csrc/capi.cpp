@@ -572,3 +572,14 @@ int nufht_b200_phase_times(double* ms, int nphase) {
 }
 
 }  // extern "C"
+
+extern "C" int nufht_b200_plan_stats(const NufhtDevicePlan* plan, double* out, int n) {
+  if (!plan || !out || n <= 0) return -400;
+  hankel::plan_stats(*plan->dp, out, n);
+  return 0;
+}
+
+extern "C" int nufht_b200_fp64_peak(double* tflops) {
+  if (!tflops) return -400;
+  return hankel::fp64_peak(tflops);
+}

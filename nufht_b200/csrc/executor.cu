@@ -285,8 +285,8 @@ void DevicePlan::build_lists() {
     d.mode = worst > kTileMaxSources ? 1 : 0;
     tmp.push_back(d);
   }
-  // Layout: groups of boxes with equal (mode, n2), mode-1 groups first so that their
-  // rows form one range to zero; within a group boxes are interleaved row by row.
+  // Layout: groups of consecutive boxes with equal (mode, n2), mode-1 groups first so that
+  // their cells form one range to zero before spreading.
   std::vector<int> order(tmp.size());
   for (size_t q = 0; q < order.size(); ++q) order[q] = (int)q;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
@@ -302,19 +302,18 @@ void DevicePlan::build_lists() {
     gr.n2 = tmp[order[q]].n2;
     gr.nbox = (int)(e - q);
     gr.mode = tmp[order[q]].mode;
-    gr.row0 = row;
+    gr.cell_off = row;
     gr.plan = 0;
     for (size_t z = q; z < e; ++z) {
       AsyBoxD d = tmp[order[z]];
-      d.row0 = row + (long long)(z - q);
-      d.rstride = gr.nbox;
+      d.cell_off = row;
       d.corr_off = coff;
       d.post_off = poff;
       coff += 2LL * d.half + 1;
       poff += d.i1 - d.i0 + 1;
+      row += d.n2;
       asyb.push_back(d);
     }
-    row += (long long)gr.n2 * gr.nbox;
     if (gr.mode == 1) chunk_cell_end = row;
     groups.push_back(gr);
     q = e;
@@ -460,8 +459,8 @@ DevicePlan::~DevicePlan() {
   if (prev >= 0) cudaSetDevice(prev);
 }
 
-// FFT plans for batch size B: group g transforms nbox * V interleaved vectors of length n2
-// (stride nbox * V, distance 1).  Plans are remade when B changes.
+// FFT plans for batch size B: group g transforms nbox * V contiguous vectors of length n2.
+// Plans are remade when B changes.
 int DevicePlan::ensure_fft(int B) {
   if (asyb.empty() || B == fft_B) return 0;
   release_fft();
@@ -477,9 +476,8 @@ int DevicePlan::ensure_fft(int B) {
       cufftDestroy(h);
       return NUFHT_E_TOO_LARGE;
     }
-    int emb = nn;
     size_t wsz = 0;
-    if (cufftMakePlanMany(h, 1, &nn, &emb, (int)batch, 1, &emb, (int)batch, 1, CUFFT_Z2Z, (int)batch, &wsz) !=
+    if (cufftMakePlanMany(h, 1, &nn, nullptr, 1, nn, nullptr, 1, nn, CUFFT_Z2Z, (int)batch, &wsz) !=
         CUFFT_SUCCESS) {
       cufftDestroy(h);
       std::fprintf(stderr, "nufht_b200: cufftMakePlanMany failed (n=%d batch=%lld)\n", nn, batch);
@@ -545,9 +543,9 @@ int launch_spread(DevicePlan& D, const AsyClass& K, const double* cs, int ld_cs,
   if (K.nspread == 0) return 0;
   const AsyLaunch L = asy_launch_shape(D, B);
   constexpr int SCP = kSpreadChunk + 1;
-  size_t sm = sizeof(double2) * spread_window(W) * L.VCTA + sizeof(double) * kSpreadChunk * W +
+  size_t sm = sizeof(double2) * spread_window(W) * (L.VCTA + 1) + sizeof(double) * kSpreadChunk * W +
               sizeof(double2) * kSpreadChunk + sizeof(double) * kSpreadChunk * D.NLP +
-              sizeof(double) * L.BT * SCP + sizeof(int) * kSpreadChunk;
+              sizeof(double) * L.BT * SCP + sizeof(double) * kSpreadChunk + sizeof(int) * kSpreadChunk;
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(k_asy_spread<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -616,7 +614,7 @@ int run_asy(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, i
     PhaseScope ps(kPhaseFft, st);
     for (const FftGroup& gr : D.groups) {
       cufftSetStream(gr.plan, st);
-      double2* p = D.d_grid + (size_t)gr.row0 * V;
+      double2* p = D.d_grid + (size_t)gr.cell_off * V;
       if (cufftExecZ2Z(gr.plan, (cufftDoubleComplex*)p, (cufftDoubleComplex*)p, CUFFT_INVERSE) != CUFFT_SUCCESS)
         return NUFHT_E_CUDA;
     }

@@ -28,19 +28,15 @@ struct DirItem { int i0, ni, j0, nj, lanes; };
 
 // Geometry of one asymptotic box's type-3 transform: sources x = r - C, targets s = k - D,
 // spreading grid spacing h (cells l in [-half, half]), FFT length n2, its rows in the
-// per-cell deconvolution and per-target phase tables, and its place in the workspace.
-// The workspace holds, per FFT group of boxes with equal n2, the cells of all its boxes
-// and all V = NLP * B vectors interleaved: element (cell q, vector v) of the box sits at
-// (row0 + q * rstride) * V + v, so neighbouring vectors are neighbouring addresses and
-// cuFFT sees nbox * V transforms with stride nbox * V and distance 1.
+// per-cell deconvolution and per-target phase tables, and its place in the workspace:
+// n2 * V contiguous complex values from cell_off * V, vector v at offset v * n2.
 struct AsyBoxD {
   int i0, i1, j0, j1;
   double C, D, h;
   int half, n2;
   int mode;             // 0: CTAs own grid tiles; 1: CTAs own source chunks (dense boxes)
   int cls;              // kernel class (oversampling and kernel width)
-  long long row0;       // first grid row of this box
-  int rstride;          // grid rows between consecutive cells of this box
+  long long cell_off;   // workspace offset in cells of one vector
   long long corr_off;   // first of 2 half + 1 entries in the cell table
   long long post_off;   // first of i1 - i0 + 1 entries in the target table
 };
@@ -54,7 +50,7 @@ struct SpreadItem {
 struct InterpItem { int box, ks, ke; };
 struct FftGroup {
   int n2, nbox, mode;
-  long long row0;  // first grid row; the group spans n2 * nbox rows
+  long long cell_off;  // the group's boxes are consecutive in the workspace
   cufftHandle plan;
 };
 
@@ -159,4 +155,12 @@ int phase_times(double* ms, int nphase);
 
 int run_besselj(double nu, const double* x, double* out, long count, cudaStream_t st);
 
+}  // namespace hankel
+
+namespace hankel {
+// Algorithmic work of a plan per batch column, for roofline accounting (see stats order in
+// nufht_b200_plan_stats).
+void plan_stats(const DevicePlan& D, double* out, int n);
+// Measured FP64 fused-multiply-add throughput of the current device in TFLOP/s.
+int fp64_peak(double* tflops);
 }  // namespace hankel

@@ -12,8 +12,8 @@
 // p = 0 add Re, p = 1 subtract Im (src/expansions.c:520-557); both are written as
 // Re(mu F) with mu rotated by i for p = 1.
 //
-// Workspace layout (see AsyBoxD): vector-interleaved rows, so thread v of a CTA always
-// touches address row * V + v and a warp's accesses are contiguous.
+// Workspace layout: box b owns n2 * V contiguous complex values, vector v = t * NLP + lp
+// at offset cell_off * V + v * n2 (one contiguous FFT input per vector).
 #pragma once
 
 #include <climits>
@@ -60,6 +60,8 @@ __global__ void k_asy_setup_targets(const double* __restrict__ ws, const AsyBoxD
 // Stage 1.  Thread (tl, lp) of the CTA owns expansion term lp of column t0 + tl, i.e.
 // vector v = t0 * NLP + tid.  Sources are sorted, so those whose kernel support starts at
 // the same cell accumulate in registers and reach the shared window once per cell change.
+// The window rows are padded by one element so that the transposed write-out (threads
+// along cells) is free of bank conflicts.
 template <int W>
 __global__ void __launch_bounds__(256) k_asy_spread(
     const double* __restrict__ rs, const double* __restrict__ cs, int ld_cs, int B,
@@ -72,29 +74,34 @@ __global__ void __launch_bounds__(256) k_asy_spread(
   const AsyBoxD bx = boxes[it.box];
   const int NLP = P.NLP;
   const int VCTA = blockDim.x;
+  const int WP = VCTA + 1;  // padded window row
   const int tid = threadIdx.x;
   const int tl = tid / NLP, lp = tid - tl * NLP;
   const int t0 = blockIdx.y * BT;
-  const int v = t0 * NLP + tid;
-  const bool active = (tl < BT) && (t0 + tl < B);
-  const size_t V = (size_t)V_total;
+  const int v0 = t0 * NLP;
+  const int nv = min(VCTA, V_total - v0);  // vectors of this CTA
+  const bool active = tid < nv;
+  double2* gbox = grid + (size_t)bx.cell_off * (size_t)V_total;
+  const int nc = it.ncell;
 
-  if (it.mode == 2) {  // zero padding of the FFT input
-    if (active)
-      for (int cell = 0; cell < it.ncell; ++cell)
-        grid[(size_t)(bx.row0 + (long long)(it.fft_start + cell) * bx.rstride) * V + v] = make_double2(0.0, 0.0);
+  if (it.mode == 2) {  // zero padding of the FFT input: threads along cells
+    for (int e = tid; e < nc * nv; e += VCTA) {
+      int vv = e / nc, cell = e - vv * nc;
+      gbox[(size_t)(v0 + vv) * bx.n2 + it.fft_start + cell] = make_double2(0.0, 0.0);
+    }
     return;
   }
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* win = reinterpret_cast<double2*>(smem_raw);                 // [WIN][VCTA]
-  double* s_w = reinterpret_cast<double*>(win + WIN * VCTA);          // [SCH][W]
+  double2* win = reinterpret_cast<double2*>(smem_raw);                 // [WIN][WP]
+  double* s_w = reinterpret_cast<double*>(win + WIN * WP);            // [SCH][W]
   double2* s_ph = reinterpret_cast<double2*>(s_w + kSpreadChunk * W); // [SCH]
   double* s_rho = reinterpret_cast<double*>(s_ph + kSpreadChunk);     // [SCH][NLP]
   double* s_c = s_rho + kSpreadChunk * NLP;                            // [BT][SCP]
-  int* s_l0 = reinterpret_cast<int*>(s_c + BT * SCP);                  // [SCH]
+  double* s_u = s_c + BT * SCP;                                        // [SCH]
+  int* s_l0 = reinterpret_cast<int*>(s_u + kSpreadChunk);              // [SCH]
 
-  for (int cell = 0; cell < it.ncell; ++cell) win[cell * VCTA + tid] = make_double2(0.0, 0.0);
+  for (int cell = 0; cell < nc; ++cell) win[cell * WP + tid] = make_double2(0.0, 0.0);
   const double ihw = 2.0 / (double)W;
   double2 acc[W];
 #pragma unroll
@@ -105,11 +112,11 @@ __global__ void __launch_bounds__(256) k_asy_spread(
 #pragma unroll
     for (int q = 0; q < W; ++q) {
       int cell = c0 + q - it.l_start;
-      if (cell >= 0 && cell < it.ncell) {
-        double2 w2 = win[cell * VCTA + tid];
+      if (cell >= 0 && cell < nc) {
+        double2 w2 = win[cell * WP + tid];
         w2.x += acc[q].x;
         w2.y += acc[q].y;
-        win[cell * VCTA + tid] = w2;
+        win[cell * WP + tid] = w2;
       }
       acc[q] = make_double2(0.0, 0.0);
     }
@@ -118,26 +125,32 @@ __global__ void __launch_bounds__(256) k_asy_spread(
   for (int s0 = it.js; s0 < it.je; s0 += kSpreadChunk) {
     const int ns = min(kSpreadChunk, it.je - s0);
     __syncthreads();  // previous round's staging fully consumed
+    // Per-source quantities, spread over all threads of the CTA.
     for (int s = tid; s < ns; s += VCTA) {
       double r = rs[s0 + s];
       double x = r - bx.C;
       double u = x / bx.h;
-      int l0 = (int)ceil(u - 0.5 * W);
-      s_l0[s] = l0;
-#pragma unroll
-      for (int q = 0; q < W; ++q) s_w[s * W + q] = es_kernel((double)(l0 + q) - u, ihw, P.beta);
+      s_u[s] = u;
+      s_l0[s] = (int)ceil(u - 0.5 * W);
       double sn, cn;
       sincos(bx.D * x, &sn, &cn);
       s_ph[s] = make_double2(cn, sn);
+    }
+    for (int e = tid; e < ns * NLP; e += VCTA) {
+      int s = e / NLP, q = e - s * NLP;
+      double r = rs[s0 + s];
       double rho = 1.0 / sqrt(r), ir = 1.0 / r;
-      for (int q = 0; q < NLP; ++q) {
-        s_rho[s * NLP + q] = rho;
-        rho *= ir;
-      }
+      for (int z = 0; z < q; ++z) rho *= ir;
+      s_rho[e] = rho;
     }
     for (int e = tid; e < ns * BT; e += VCTA) {
       int tt = e / ns, s = e - tt * ns;
       s_c[tt * SCP + s] = (t0 + tt < B) ? cs[(size_t)(t0 + tt) * ld_cs + s0 + s] : 0.0;
+    }
+    __syncthreads();
+    for (int e = tid; e < ns * W; e += VCTA) {
+      int s = e / W, q = e - s * W;
+      s_w[e] = es_kernel((double)(s_l0[s] + q) - s_u[s], ihw, P.beta);
     }
     __syncthreads();
     if (active) {
@@ -159,27 +172,28 @@ __global__ void __launch_bounds__(256) k_asy_spread(
       }
     }
   }
-  if (!active) return;
-  if (cur != INT_MIN) flush(cur);
-  // Each thread writes its own vector's cells: neighbouring threads, neighbouring addresses.
+  if (active && cur != INT_MIN) flush(cur);
+  __syncthreads();
+  // Transposed write-out: consecutive threads take consecutive cells of one vector.
   if (it.mode == 0) {
     // Plain stores: this CTA owns cells [l_start, l_start + ncell) of the box.
-    for (int cell = 0; cell < it.ncell; ++cell) {
-      double2 val = win[cell * VCTA + tid];
+    for (int e = tid; e < nc * nv; e += VCTA) {
+      int vv = e / nc, cell = e - vv * nc;
+      double2 val = win[cell * WP + vv];
       double c = corr[bx.corr_off + it.l_start + cell + bx.half];
-      grid[(size_t)(bx.row0 + (long long)(it.fft_start + cell) * bx.rstride) * V + v] =
-          make_double2(val.x * c, val.y * c);
+      gbox[(size_t)(v0 + vv) * bx.n2 + it.fft_start + cell] = make_double2(val.x * c, val.y * c);
     }
   } else {
     // Atomic adds into the (pre-zeroed) grid of a dense box.
-    for (int cell = 0; cell < it.ncell; ++cell) {
+    for (int e = tid; e < nc * nv; e += VCTA) {
+      int vv = e / nc, cell = e - vv * nc;
       int l = it.l_start + cell;
       if (l < -bx.half || l > bx.half) continue;
-      double2 val = win[cell * VCTA + tid];
+      double2 val = win[cell * WP + vv];
       if (val.x == 0.0 && val.y == 0.0) continue;
       double c = corr[bx.corr_off + l + bx.half];
       int idx = l < 0 ? l + bx.n2 : l;
-      double* dst = reinterpret_cast<double*>(grid + (size_t)(bx.row0 + (long long)idx * bx.rstride) * V + v);
+      double* dst = reinterpret_cast<double*>(gbox + (size_t)(v0 + vv) * bx.n2 + idx);
       atomicAdd(dst, val.x * c);
       atomicAdd(dst + 1, val.y * c);
     }
@@ -211,9 +225,8 @@ __global__ void __launch_bounds__(256) k_asy_interp(
   int* s_q0 = reinterpret_cast<int*>(s_y + kInterpChunk * VCTA);        // [KC]
 
   const int n2 = bx.n2;
-  const size_t V = (size_t)V_total;
-  const size_t rowstep = (size_t)bx.rstride * V;
-  const double2* base = grid + (size_t)bx.row0 * V + (size_t)(t0 * NLP + tid);
+  const double2* row =
+      grid + (size_t)bx.cell_off * (size_t)V_total + (size_t)(t0 * NLP + tid) * (size_t)n2;
   const double ihw = 2.0 / (double)W;
   const double u_scale = bx.h * (double)n2 / (2.0 * M_PI);
   double2 g[W];
@@ -249,13 +262,13 @@ __global__ void __launch_bounds__(256) k_asy_interp(
             for (int q = 0; q < W - 1; ++q) g[q] = g[q + 1];
             int idx = q0 + W - 1;
             idx = idx < 0 ? idx + n2 : (idx >= n2 ? idx - n2 : idx);
-            g[W - 1] = base[(size_t)idx * rowstep];
+            g[W - 1] = row[idx];
           } else {
 #pragma unroll
             for (int q = 0; q < W; ++q) {
               int idx = q0 + q;
               idx = idx < 0 ? idx + n2 : (idx >= n2 ? idx - n2 : idx);
-              g[q] = base[(size_t)idx * rowstep];
+              g[q] = row[idx];
             }
           }
           gq = q0;

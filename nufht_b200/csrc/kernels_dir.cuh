@@ -39,7 +39,18 @@ __global__ void __launch_bounds__(kDirThreads) k_dir(
     }
     __syncthreads();
     if (valid) {
-      for (int s = lane; s < ns; s += L) {
+      // Two independent Bessel evaluations per step for instruction-level parallelism.
+      int s = lane;
+      for (; s + L < ns; s += 2 * L) {
+        double Ja = bessel_j(nu2, k * s_r[s]);
+        double Jb = bessel_j(nu2, k * s_r[s + L]);
+#pragma unroll
+        for (int q = 0; q < BT; ++q) {
+          acc[q] = fma(s_c[q * kDirChunk + s], Ja, acc[q]);
+          acc[q] = fma(s_c[q * kDirChunk + s + L], Jb, acc[q]);
+        }
+      }
+      if (s < ns) {
         double J = bessel_j(nu2, k * s_r[s]);
 #pragma unroll
         for (int q = 0; q < BT; ++q) acc[q] = fma(s_c[q * kDirChunk + s], J, acc[q]);

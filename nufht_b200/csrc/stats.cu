@@ -1,0 +1,84 @@
+// Workload statistics of a plan and an FP64 throughput probe, used by the benchmark to
+// express kernel times as fractions of a roofline.
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "executor.h"
+
+namespace hankel {
+
+// out[0]  sum over asymptotic boxes of sources (nj)
+// out[1]  sum over asymptotic boxes of targets (ni)
+// out[2]  FFT cells (sum of n2)
+// out[3]  sum of nj * W (spreading taps per vector)
+// out[4]  sum of ni * W (interpolation taps per vector)
+// out[5]  direct-box pairs (sum of ni * nj)
+// out[6]  local boxes: sum of nj
+// out[7]  local boxes: sum of ni
+// out[8]  FFT cells read by interpolation (sum of n2 / sigma + W)
+// out[9]  FFT flops per vector (sum of 5 n2 log2 n2)
+// out[10] expansion terms per column (NLP)
+// out[11] local expansion terms (K_loc + 1)
+void plan_stats(const DevicePlan& D, double* out, int n) {
+  double s[12] = {0};
+  for (const AsyBoxD& b : D.asyb) {
+    double nj = b.j1 - b.j0 + 1, ni = b.i1 - b.i0 + 1;
+    const AsyClass& K = D.classes[b.cls];
+    s[0] += nj;
+    s[1] += ni;
+    s[2] += b.n2;
+    s[3] += nj * K.W;
+    s[4] += ni * K.W;
+    s[8] += std::min((double)b.n2, b.n2 / K.sigma + K.W);
+    s[9] += 5.0 * b.n2 * std::log2((double)b.n2);
+  }
+  for (const HBox& b : D.dir_boxes) s[5] += (double)(b.i1 - b.i0 + 1) * (double)(b.j1 - b.j0 + 1);
+  for (const HBox& b : D.loc_boxes) {
+    s[6] += b.j1 - b.j0 + 1;
+    s[7] += b.i1 - b.i0 + 1;
+  }
+  s[10] = D.NLP;
+  s[11] = D.KL1;
+  for (int i = 0; i < n && i < 12; ++i) out[i] = s[i];
+}
+
+namespace {
+__global__ void k_fp64_fma(double* out, int iters, double a, double b) {
+  double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  for (int i = 0; i < iters; ++i) {
+    x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+    x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+  }
+  double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == 12345.678) out[0] = s;  // keeps the loop alive
+}
+}  // namespace
+
+int fp64_peak(double* tflops) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  double* d = nullptr;
+  if (cudaMalloc(&d, sizeof(double)) != cudaSuccess) return NUFHT_E_CUDA;
+  const int blocks = sms * 8, threads = 256, iters = 4096;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  k_fp64_fma<<<blocks, threads>>>(d, 64, 0.999999, 1e-9);  // warm up
+  cudaEventRecord(e0);
+  k_fp64_fma<<<blocks, threads>>>(d, iters, 0.999999, 1e-9);
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  if (cudaGetLastError() != cudaSuccess || ms <= 0.f) return NUFHT_E_CUDA;
+  double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return 0;
+}
+
+}  // namespace hankel

@@ -325,11 +325,17 @@ static void o_fft_pos(double *a, int n) /* in place, sum_l a_l e^{+2 pi i q l / 
             a[2 * j] = tr; a[2 * j + 1] = ti;
         }
     }
+    /* twiddles exp(2 pi i k / n), k < n/2, computed once */
+    double *tw = (double *)malloc(sizeof(double) * (size_t)(n > 1 ? n : 2));
+    for (int k = 0; k < n / 2; ++k) {
+        tw[2 * k] = cos(2.0 * M_PI * k / n);
+        tw[2 * k + 1] = sin(2.0 * M_PI * k / n);
+    }
     for (int len = 2; len <= n; len <<= 1) {
-        double ang = 2.0 * M_PI / len;
+        int step = n / len;
         for (int i = 0; i < n; i += len) {
             for (int k = 0; k < len / 2; ++k) {
-                double wr = cos(ang * k), wi = sin(ang * k);
+                double wr = tw[2 * k * step], wi = tw[2 * k * step + 1];
                 double *u = a + 2 * (i + k), *v = a + 2 * (i + k + len / 2);
                 double vr = v[0] * wr - v[1] * wi, vi = v[0] * wi + v[1] * wr;
                 v[0] = u[0] - vr; v[1] = u[1] - vi;
@@ -337,6 +343,7 @@ static void o_fft_pos(double *a, int n) /* in place, sum_l a_l e^{+2 pi i q l / 
             }
         }
     }
+    free(tw);
 }
 
 static double o_es(double u, int w, double beta) /* ES kernel in grid units, support |u|<w/2 */
@@ -645,6 +652,46 @@ void oracle_add_asy_batch(double *gs, double nu, const double *rs, const double 
     double s2p = sqrt(2.0 / M_PI);
     double pa = M_PI * (-nu / 2.0 - 0.25);
     double pr = cos(pa), pi_ = sin(pa);
+    if (g_t3_mode == ORACLE_T3_NUFFT && g_threads > 1 && K >= 0) {
+        /* Parallel over the 2(K+1) independent transforms (the reference runs them one after
+         * another); the terms are added to gs in the reference's order. */
+        int nq = 2 * (K + 1), err = 0;
+        double *terms = (double *)malloc(sizeof(double) * (size_t)nq * n * batch);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(g_threads) reduction(| : err)
+        for (int q = 0; q < nq; ++q) {
+            int l = q / 2, half = q & 1;
+            int e = half == 0 ? -2 * l - 1 : -2 * l - 2;
+            double *ci = (double *)malloc(sizeof(double) * 2 * (size_t)m * batch);
+            double *co = (double *)malloc(sizeof(double) * 2 * (size_t)n * batch);
+            for (int t = 0; t < batch; ++t)
+                for (int k = 0; k < m; ++k) {
+                    double rk = rs[k];
+                    ci[2 * ((size_t)t * m + k)] = cs[(size_t)t * ld_cs + k] * pow(rk, (double)e) * sqrt(rk);
+                    ci[2 * ((size_t)t * m + k) + 1] = 0.0;
+                }
+            err |= o_type3_nufft(batch, m, rs, ci, tol, n, ws, co);
+            double sl = (l & 1) ? -1.0 : 1.0;
+            double coeff = s2p * sl * asy_coef[2 * l + half];
+            double *tq = terms + (size_t)q * n * batch;
+            for (int t = 0; t < batch; ++t)
+                for (int j = 0; j < n; ++j) {
+                    double wj = ws[j];
+                    double sc = coeff * pow(wj, (double)e) * sqrt(wj);
+                    double fr = co[2 * ((size_t)t * n + j)], fi = co[2 * ((size_t)t * n + j) + 1];
+                    double vr = fr * pr - fi * pi_, vi = fr * pi_ + fi * pr;
+                    tq[(size_t)t * n + j] = half == 0 ? vr * sc : -vi * sc;
+                }
+            free(ci);
+            free(co);
+        }
+        if (err) fprintf(stderr, "oracle add_asy_batch: type-3 failed\n");
+        for (int q = 0; q < nq; ++q)
+            for (int t = 0; t < batch; ++t)
+                for (int j = 0; j < n; ++j) gs[(size_t)t * ld_gs + j] += terms[((size_t)q * batch + t) * n + j];
+        free(terms);
+        if (own) { free(cin); free(cout); }
+        return;
+    }
     for (int l = 0; l <= K; ++l) {
         for (int half = 0; half < 2; ++half) {
             int e = half == 0 ? -2 * l - 1 : -2 * l - 2;
