@@ -230,6 +230,20 @@ int nufht_b200_plan_stats(const NufhtDevicePlan *plan, double *out, int n);
 /* Measured FP64 fused-multiply-add throughput of the current device (TFLOP/s). */
 int nufht_b200_fp64_peak(double *tflops);
 
+/* No counterpart in the reference.  Allocation-free variant of add_loc_batch for callers
+ * that cannot call cudaMalloc at call time (a fixed memory budget or pool, allocation
+ * forbidden after start-up): adds the local (Wimp) expansion of the single box
+ * [0,n) x [0,m) to gs, with its scratch (work lists, partial projections, coefficients) in
+ * a 4 MiB device array inside the library that every GPU loading the library holds until
+ * exit.  gs, rs, cs, ws are DEVICE pointers; nu is an integer order; asynchronous on
+ * `stream`.  Returns 0, -400/-401 (arguments), -2 (order), NUFHT_E_TOO_LARGE when the
+ * scratch would exceed 4 MiB (about ceil(m/2048) (K+1) batch 8 bytes plus work lists),
+ * NUFHT_E_CUDA.  The first call on a device looks up the array's address and should come
+ * before any stream capture; calls that overlap on the GPU share the array and race. */
+int nufht_b200_add_loc_batch_noalloc(double *gs, double nu, const double *rs, const double *cs,
+                                     const double *ws, int m, int n, int K, int batch, int ld_cs,
+                                     int ld_gs, void *stream);
+
 /* Where the planning tables were read from (a cache file path), or "generated". */
 const char *nufht_b200_table_source(void);
 

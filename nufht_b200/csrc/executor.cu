@@ -706,6 +706,39 @@ int DevicePlan::run(const double* cs, int ld_cs, double* gs, int ld_gs, int B, c
   return 0;
 }
 
+// The local-expansion kernels of one box on caller-provided device buffers (work lists,
+// partial projections and coefficients), without any allocation; g += the box's
+// contribution.  Used by the allocation-free entry point (noalloc.cu).
+int run_loc_box(const double* rs, const double* ws, const double* cs, int ld_cs, double* gs, int ld_gs,
+                int B, const LocBoxD* d_box, const ProjItem* d_proj, int nproj, const EvalItem* d_eval,
+                int neval, double* d_partial, double* d_cheb, int K, int nu_int, cudaStream_t st) {
+  const int KL1 = K + 1;
+  if (KL1 > 256) return NUFHT_E_TOO_LARGE;
+  int BT = 32;
+  while (BT > 1 && KL1 * BT > 256) BT >>= 1;
+  BT = std::min(BT, B);
+  size_t sm = sizeof(double) * (KL1 * kLocChunk + kLocChunk * BT);
+  if (sm > 48 * 1024) cudaFuncSetAttribute(k_loc_proj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_loc_proj<<<dim3((unsigned)nproj, (unsigned)((B + BT - 1) / BT)), 256, sm, st>>>(
+      rs, cs, ld_cs, B, d_box, d_proj, KL1, nu_int & 1, d_partial, BT);
+  NUFHT_LAUNCH_CHECK();
+  long long tot = (long long)KL1 * B;
+  k_loc_reduce<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_box, 1, KL1, B, d_partial, d_cheb);
+  NUFHT_LAUNCH_CHECK();
+  const int maxo = nu_int / 2 + K + (nu_int & 1);
+  size_t sme = sizeof(double) * KL1 * B;
+  auto eval = [&](auto kern) -> int {
+    if (sme > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sme);
+    kern<<<(unsigned)neval, kLocTargets, sme, st>>>(ws, gs, ld_gs, B, d_box, d_eval, d_cheb, K, nu_int, 1.0);
+    NUFHT_LAUNCH_CHECK();
+    return 0;
+  };
+  if (maxo <= 64) return eval(k_loc_eval<64>);
+  if (maxo <= 160) return eval(k_loc_eval<160>);
+  if (maxo <= 512) return eval(k_loc_eval<512>);
+  return NUFHT_E_TOO_LARGE;
+}
+
 int run_besselj(double nu, const double* x, double* out, long count, cudaStream_t st) {
   double anu = std::fabs(nu);
   int nu2 = (int)std::llround(2.0 * anu);

@@ -164,3 +164,9 @@ void plan_stats(const DevicePlan& D, double* out, int n);
 // Measured FP64 fused-multiply-add throughput of the current device in TFLOP/s.
 int fp64_peak(double* tflops);
 }  // namespace hankel
+
+namespace hankel {
+int run_loc_box(const double* rs, const double* ws, const double* cs, int ld_cs, double* gs, int ld_gs,
+                int B, const LocBoxD* d_box, const ProjItem* d_proj, int nproj, const EvalItem* d_eval,
+                int neval, double* d_partial, double* d_cheb, int K, int nu_int, cudaStream_t st);
+}  // namespace hankel
