@@ -192,7 +192,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--n", type=int, default=1000000)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -277,6 +277,36 @@ def main():
         ms = float(t.item())
     value = 2.0 * (N + M) * B * world / (ms * 1e-3) / 1e9
 
+    # The plain FP64 form of the same method on the same inputs, for the mixed/FP64 ratio.
+    fp64 = None
+    if mixed:
+        qf = DevicePlan(0.0, r, k, tol, mixed=False, device=local)
+        qa = DevicePlan(0.0, k, r, tol, mixed=False, device=local)
+
+        def step64():
+            qf.execute_columns(c, g, st)
+            qa.execute_columns(y, h, st)
+
+        for _ in range(max(args.warmup, 3)):
+            step64()
+        barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(st)
+        for _ in range(args.steps):
+            step64()
+        f1.record(st)
+        barrier()
+        ms64 = f0.elapsed_time(f1) / args.steps
+        if pg:
+            t = torch.tensor([ms64], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms64 = float(t.item())
+        fp64 = {"value": 2.0 * (N + M) * B * world / (ms64 * 1e-3) / 1e9, "ms_per_step": ms64,
+                "mixed_over_fp64": ms64 / ms}
+        qf.close()
+        qa.close()
+
     # Per-kernel device times over a second run of the same steps (CUDA events on the
     # launching stream around each phase), for the roofline of the dominant kernel.
     lib.nufht_b200_set_phase_timing(1)
@@ -287,7 +317,9 @@ def main():
     phases = {kk: v / args.steps for kk, v in L.phase_times().items()}
 
     # End to end through the reference-facing C ABI: nufht_plan_init / nufht_batch with host
-    # buffers (pinned), the copies inside the timed region.
+    # buffers (pinned), the copies inside the timed region.  The precision of that entry
+    # point is chosen with NUFHT_B200_PRECISION (read when a plan first runs).
+    os.environ["NUFHT_B200_PRECISION"] = "mixed" if mixed else "fp64"
     plans = []
     for (a, b) in ((r, k), (k, r)):
         p = L.NufhtPlan()
@@ -331,10 +363,11 @@ def main():
     lib.nufht_b200_plan_stats(pf._h, sf.ctypes.data_as(L.c_double_p), 12)
     lib.nufht_b200_plan_stats(pa._h, sa.ctypes.data_as(L.c_double_p), 12)
     V = sf[10] * B
-    byts = {  # algorithmic bytes per fwd+adj step (both plans), FP64 storage
-        "asy_spread": sum(8.0 * s[0] * (B + 1) + 16.0 * s[2] * V for s in (sf, sa)),
-        "asy_fft": sum(2 * 16.0 * s[2] * V for s in (sf, sa)),
-        "asy_interp": sum(16.0 * s[8] * V + 8.0 * s[1] * (2 * B + 1) for s in (sf, sa)),
+    gb = 8.0 if mixed else 16.0  # bytes per complex grid value (FP32 / FP64)
+    byts = {  # algorithmic bytes per fwd+adj step (both plans)
+        "asy_spread": sum(8.0 * s[0] * (B + 1) + gb * s[2] * V for s in (sf, sa)),
+        "asy_fft": sum(2 * gb * s[2] * V for s in (sf, sa)),
+        "asy_interp": sum(gb * s[8] * V + 8.0 * s[1] * (2 * B + 1) for s in (sf, sa)),
     }
     flops = {
         "asy_spread": sum(4.0 * s[3] * V for s in (sf, sa)),
@@ -344,8 +377,8 @@ def main():
     dom = max(phases, key=lambda kk: phases[kk])
     kname = {"asy_spread": "k_asy_spread", "asy_interp": "k_asy_interp", "asy_fft": "cufft",
              "dir": "k_dir", "loc_proj": "k_loc_proj", "loc_eval": "k_loc_eval", "zero": "memset"}[dom]
-    fp64 = ctypes.c_double(0.0)
-    lib.nufht_b200_fp64_peak(ctypes.byref(fp64))
+    fp64_peak = ctypes.c_double(0.0)
+    lib.nufht_b200_fp64_peak(ctypes.byref(fp64_peak))
     t_dom = phases[dom] * 1e-3  # per step (2 launches: forward and adjoint plan)
     ach_gbs = byts.get(dom, 0.0) / t_dom / 1e9 if t_dom > 0 else 0.0
     roofline = {"kernel": kname, "bound": "hbm", "achieved": ach_gbs, "peak": hbm, "unit": "GB/s",
@@ -354,10 +387,10 @@ def main():
                 "traffic": traffic_from_profiles(kname),
                 "algorithmic_bytes_per_launch": byts.get(dom, 0.0) / 2,
                 "avg_launch_ms": phases[dom] / 2}
-    if dom in flops:
+    if dom in flops and (not mixed or dom == "dir"):
         ach_tf = flops[dom] / t_dom / 1e12
-        roofline["fp64"] = {"achieved": ach_tf, "peak": fp64.value, "unit": "TFLOP/s",
-                            "frac": ach_tf / fp64.value if fp64.value > 0 else None,
+        roofline["fp64"] = {"achieved": ach_tf, "peak": fp64_peak.value, "unit": "TFLOP/s",
+                            "frac": ach_tf / fp64_peak.value if fp64_peak.value > 0 else None,
                             "peak_source": "measured FP64 FMA probe (nufht_b200_fp64_peak)"}
 
     cpu = None
@@ -375,7 +408,7 @@ def main():
                 "data": "synthetic (seeded numpy draws with the workload's shapes)", "config": config,
                 "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches),
                 "phases_ms_per_step": phases, "roofline": roofline, "cpu_baseline": cpu,
-                "plan": pf.info()}
+                "fp64_form": fp64, "plan": pf.info()}
         print(json.dumps(line))
     pf.close()
     pa.close()

@@ -180,6 +180,7 @@ typedef struct {
     int spread_width;              /* exponential-of-semicircle kernel width */
     int path;                      /* 0 boxes, 1 all-direct, 2 all-asymptotic (half-integer) */
     size_t workspace_bytes;        /* device workspace for the last batch size executed */
+    int mixed;                     /* 1 when the asymptotic boxes run in FP32 */
 } NufhtB200Info;
 
 /* Build a device plan.  rs (m) and ws (n) may be host or device pointers; they are

@@ -51,7 +51,8 @@ class NufhtB200Info(ctypes.Structure):
     _fields_ = [("nu", ctypes.c_double), ("tol", ctypes.c_double), ("z_split", ctypes.c_double),
                 ("K_asy", ctypes.c_int), ("K_loc", ctypes.c_int), ("n_loc", ctypes.c_long),
                 ("n_asy", ctypes.c_long), ("n_dir", ctypes.c_long), ("fft_points", ctypes.c_long),
-                ("spread_width", ctypes.c_int), ("path", ctypes.c_int), ("workspace_bytes", ctypes.c_size_t)]
+                ("spread_width", ctypes.c_int), ("path", ctypes.c_int), ("workspace_bytes", ctypes.c_size_t),
+                ("mixed", ctypes.c_int)]
 
 
 NUFHT_B200_FP64 = 0x0

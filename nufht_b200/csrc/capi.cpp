@@ -148,6 +148,10 @@ int device_state_for(const NufhtPlan* plan, DevicePlan** out) {
   D->plan_loc = to_hbox(plan->boxes.loc);
   D->plan_asy = to_hbox(plan->boxes.asy);
   D->plan_dir = to_hbox(plan->boxes.dir);
+  // The reference's entry points carry no precision argument; NUFHT_B200_PRECISION=mixed
+  // selects the mixed-precision asymptotic path for them (same rule as NUFHT_B200_MIXED).
+  if (const char* pr = std::getenv("NUFHT_B200_PRECISION"))
+    D->mixed_asy = std::strcmp(pr, "mixed") == 0 && D->P.tol >= 1e-9;
   choose_path(D.get(), plan->min_dim_prod);
   int dev = 0;
   cudaGetDevice(&dev);
@@ -470,6 +474,9 @@ int nufht_b200_plan_create(NufhtDevicePlan** out, double nu, const double* rs, i
   D->m = m;
   D->n = n;
   D->flags = flags;
+  // Mixed precision: the asymptotic boxes (the bulk of the work) run in FP32; below
+  // tol = 1e-9 single precision cannot reach the requested accuracy and FP64 is kept.
+  D->mixed_asy = (flags & NUFHT_B200_MIXED) != 0 && D->P.tol >= 1e-9;
   if ((rc = host_copy(rs, m, &D->h_rs)) || (rc = host_copy(ws, n, &D->h_ws))) return rc;
   if (hankel::check_grid(D->h_rs.data(), m)) return NUFHT_E_UNSORTED_RS;
   if (hankel::check_grid(D->h_ws.data(), n)) return NUFHT_E_UNSORTED_WS;
@@ -512,6 +519,7 @@ int nufht_b200_plan_info(const NufhtDevicePlan* plan, NufhtB200Info* info) {
   info->spread_width = D->W;
   info->path = D->path;
   info->workspace_bytes = D->ws_bytes;
+  info->mixed = D->mixed_asy ? 1 : 0;
   return 0;
 }
 

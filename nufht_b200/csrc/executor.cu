@@ -229,6 +229,9 @@ void DevicePlan::build_lists() {
   NLP = 2 * (P.K_asy + 1);
   int Wc[3];
   for (int c = 0; c < 3; ++c) Wc[c] = spread_width(P.tol, kSigmas[c]);
+  // In FP32 the deconvolution by psi-hat amplifies rounding by psi-hat(0)/psi-hat(pi/sigma):
+  // about 3 at sigma = 2, 26 at 1.5 and 1100 at 1.25, so mixed precision keeps sigma = 2.
+  if (mixed_asy) Wc[1] = Wc[2] = 0;
   std::vector<AsyBoxD> tmp;
   for (const HBox& hb : asy_boxes) {
     AsyBoxD d;
@@ -239,6 +242,12 @@ void DevicePlan::build_lists() {
     d.j1 = hb.j1;
     double rlo = rs[hb.j0], rhi = rs[hb.j1], klo = ws[hb.i0], khi = ws[hb.i1];
     d.C = 0.5 * (rlo + rhi);
+    // smallest positive radius of the box (sources at r = 0 contribute nothing here:
+    // J_nu(0) = 0 for every order that reaches an asymptotic box)
+    {
+      const double* p = std::upper_bound(rs + hb.j0, rs + hb.j1 + 1, 0.0);
+      d.rref = p <= rs + hb.j1 ? *p : 1.0;
+    }
     double X = 0.5 * (rhi - rlo);
     d.D = 0.5 * (klo + khi);
     double S = 0.5 * (khi - klo);
@@ -321,7 +330,9 @@ void DevicePlan::build_lists() {
   total_cells = row;
   total_corr = coff;
   total_post = poff;
-  // Work items, grouped by kernel class.
+  // Work items, grouped by kernel class: windowed spreading items (mode 0 tiles and mode 2
+  // zero padding), then atomic ones (mode 1 chunks of dense boxes).
+  std::vector<SpreadItem> atomic_items;
   for (int c = 0; c < 3; ++c) {
     AsyClass K;
     K.sigma = kSigmas[c];
@@ -372,32 +383,27 @@ void DevicePlan::build_lists() {
           spread.push_back(s);
         }
       } else {
-        // Source chunks of at most kChunkSources whose supports (plus one cell of margin
-        // on either side) fit the window of spread_window(W) cells.
-        const int winc = spread_window(Wb);
-        int js = d.j0;
-        while (js <= d.j1) {
-          long long lfirst = l0_of(js);
-          long long lim = lfirst + winc - Wb - 2;  // largest start cell in this chunk
-          int je = std::min(js + kChunkSources, first_ge(lim + 1));
-          if (je <= js) je = js + 1;
-          long long llast = l0_of(je - 1);
+        // Dense box: chunks of kChunkSources sources, added atomically to the grid.
+        for (int js = d.j0; js <= d.j1; js += kChunkSources) {
           SpreadItem s;
           s.box = (int)b;
           s.mode = 1;
-          s.l_start = (int)(lfirst - 1);
-          s.ncell = (int)(llast + Wb + 1 - s.l_start);
+          s.l_start = 0;
+          s.ncell = 0;
           s.fft_start = 0;
           s.js = js;
-          s.je = je;
-          spread.push_back(s);
-          js = je;
+          s.je = std::min(js + kChunkSources, d.j1 + 1);
+          atomic_items.push_back(s);
         }
       }
       for (int i = d.i0; i <= d.i1; i += kInterpTile)
         interp.push_back({(int)b, i, std::min(i + kInterpTile, d.i1 + 1)});
     }
     K.nspread = (int)spread.size() - K.spread0;
+    K.spreadA0 = (int)spread.size();
+    spread.insert(spread.end(), atomic_items.begin(), atomic_items.end());
+    K.nspreadA = (int)atomic_items.size();
+    atomic_items.clear();
     K.ninterp = (int)interp.size() - K.interp0;
     if (any) K.ac = make_asy_const(P, NLP, K.W, es_beta(K.sigma, K.W));
     else std::memset(&K.ac, 0, sizeof(K.ac));
@@ -477,7 +483,7 @@ int DevicePlan::ensure_fft(int B) {
       return NUFHT_E_TOO_LARGE;
     }
     size_t wsz = 0;
-    if (cufftMakePlanMany(h, 1, &nn, nullptr, 1, nn, nullptr, 1, nn, CUFFT_Z2Z, (int)batch, &wsz) !=
+    if (cufftMakePlanMany(h, 1, &nn, nullptr, 1, nn, nullptr, 1, nn, mixed_asy ? CUFFT_C2C : CUFFT_Z2Z, (int)batch, &wsz) !=
         CUFFT_SUCCESS) {
       cufftDestroy(h);
       std::fprintf(stderr, "nufht_b200: cufftMakePlanMany failed (n=%d batch=%lld)\n", nn, batch);
@@ -506,7 +512,7 @@ int DevicePlan::ensure_workspace(int B) {
   size_t bytes = 0;
   const long long V = (long long)NLP * B;
   if (!asyb.empty()) {
-    size_t g = (size_t)total_cells * (size_t)V * sizeof(double2);
+    size_t g = (size_t)total_cells * (size_t)V * (mixed_asy ? sizeof(float2) : sizeof(double2));
     NUFHT_CUDA_TRY(cudaMalloc((void**)&d_grid, g));
     bytes += g;
   }
@@ -526,87 +532,102 @@ int DevicePlan::ensure_workspace(int B) {
 namespace {
 
 struct AsyLaunch {
-  int BT, VCTA, V_total, ngy;
+  int BTH, BT, VCTA, V_total, ngy;
 };
 
-AsyLaunch asy_launch_shape(const DevicePlan& D, int B) {
+// CTA shape with VPT vectors per thread: BTH column slots (NLP * BTH threads, at most
+// 256), BT = VPT * BTH columns per CTA.
+AsyLaunch asy_launch_shape(const DevicePlan& D, int B, int VPT) {
   AsyLaunch L;
-  L.BT = std::min(std::max(1, std::min(256 / D.NLP, 32)), B);
-  L.VCTA = D.NLP * L.BT;
+  int cap = std::max(1, std::min(256 / D.NLP, 32));
+  L.BTH = std::min(cap, (B + VPT - 1) / VPT);
+  L.BT = L.BTH * VPT;
+  L.VCTA = D.NLP * L.BTH;
   L.V_total = D.NLP * B;
   L.ngy = (B + L.BT - 1) / L.BT;
   return L;
 }
 
-template <int W>
-int launch_spread(DevicePlan& D, const AsyClass& K, const double* cs, int ld_cs, int B, cudaStream_t st) {
-  if (K.nspread == 0) return 0;
-  const AsyLaunch L = asy_launch_shape(D, B);
-  constexpr int SCP = kSpreadChunk + 1;
-  size_t sm = sizeof(double2) * spread_window(W) * (L.VCTA + 1) + sizeof(double) * kSpreadChunk * W +
-              sizeof(double2) * kSpreadChunk + sizeof(double) * kSpreadChunk * D.NLP +
-              sizeof(double) * L.BT * SCP + sizeof(double) * kSpreadChunk + sizeof(int) * kSpreadChunk;
+template <typename T, int W, bool WINDOWED>
+int launch_spread_kind(DevicePlan& D, const AsyClass& K, int item0, int nitems, const double* cs, int ld_cs,
+                       int B, cudaStream_t st) {
+  if (nitems == 0) return 0;
+  const AsyLaunch L = asy_launch_shape(D, B, 1);
+  size_t sm = spread_smem<T>(W, L.VCTA, D.NLP, L.BT, WINDOWED).total;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(k_asy_spread<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_asy_spread<T, W, WINDOWED>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     attr_set = true;
   }
-  dim3 g((unsigned)K.nspread, (unsigned)L.ngy);
-  k_asy_spread<W><<<g, L.VCTA, sm, st>>>(D.d_rs, cs, ld_cs, B, D.d_grid, D.d_asyb, D.d_spread + K.spread0,
-                                         D.d_corr, K.ac, L.BT, L.V_total);
+  dim3 g((unsigned)nitems, (unsigned)L.ngy);
+  k_asy_spread<T, W, WINDOWED><<<g, L.VCTA, sm, st>>>(D.d_rs, cs, ld_cs, B, (typename Cplx<T>::type*)D.d_grid,
+                                                      D.d_asyb, D.d_spread + item0, D.d_corr, K.ac, L.BT,
+                                                      L.V_total);
   NUFHT_LAUNCH_CHECK();
   return 0;
 }
 
-template <int W>
+template <typename T, int W>
+int launch_spread(DevicePlan& D, const AsyClass& K, const double* cs, int ld_cs, int B, cudaStream_t st) {
+  int rc = launch_spread_kind<T, W, true>(D, K, K.spread0, K.nspread, cs, ld_cs, B, st);
+  if (rc) return rc;
+  return launch_spread_kind<T, W, false>(D, K, K.spreadA0, K.nspreadA, cs, ld_cs, B, st);
+}
+
+template <typename T, int W>
 int launch_interp(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, int B, cudaStream_t st, double sgn) {
   if (K.ninterp == 0) return 0;
-  const AsyLaunch L = asy_launch_shape(D, B);
-  size_t sm = sizeof(double2) * kInterpChunk * D.NLP + sizeof(double) * kInterpChunk * W +
-              sizeof(double) * kInterpChunk * L.VCTA + sizeof(int) * kInterpChunk;
+  constexpr int VPT = interp_vpt(W);
+  const AsyLaunch L = asy_launch_shape(D, B, VPT);
+  size_t sm = sizeof(double2) * kInterpChunk * D.NLP + sizeof(double) * kInterpChunk * (L.VCTA * VPT + 1) +
+              sizeof(T) * kInterpChunk * W + sizeof(int) * kInterpChunk;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(k_asy_interp<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_asy_interp<T, W, VPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     attr_set = true;
   }
   dim3 g((unsigned)K.ninterp, (unsigned)L.ngy);
-  k_asy_interp<W><<<g, L.VCTA, sm, st>>>(D.d_ws, gs, ld_gs, B, D.d_grid, D.d_asyb, D.d_interp + K.interp0,
-                                         D.d_post, K.ac, L.BT, L.V_total, sgn);
+  k_asy_interp<T, W, VPT><<<g, L.VCTA, sm, st>>>(D.d_ws, gs, ld_gs, B, (const typename Cplx<T>::type*)D.d_grid,
+                                                 D.d_asyb, D.d_interp + K.interp0, D.d_post, K.ac, L.BTH,
+                                                 L.V_total, sgn);
   NUFHT_LAUNCH_CHECK();
   return 0;
 }
 
-#define NUFHT_W_DISPATCH(FN, Wv, ...)          \
-  switch (Wv) {                                \
-    case 2: rc = FN<2>(__VA_ARGS__); break;    \
-    case 3: rc = FN<3>(__VA_ARGS__); break;    \
-    case 4: rc = FN<4>(__VA_ARGS__); break;    \
-    case 5: rc = FN<5>(__VA_ARGS__); break;    \
-    case 6: rc = FN<6>(__VA_ARGS__); break;    \
-    case 7: rc = FN<7>(__VA_ARGS__); break;    \
-    case 8: rc = FN<8>(__VA_ARGS__); break;    \
-    case 9: rc = FN<9>(__VA_ARGS__); break;    \
-    case 10: rc = FN<10>(__VA_ARGS__); break;  \
-    case 11: rc = FN<11>(__VA_ARGS__); break;  \
-    case 12: rc = FN<12>(__VA_ARGS__); break;  \
-    case 13: rc = FN<13>(__VA_ARGS__); break;  \
-    case 14: rc = FN<14>(__VA_ARGS__); break;  \
-    case 15: rc = FN<15>(__VA_ARGS__); break;  \
-    default: rc = FN<16>(__VA_ARGS__); break;  \
+#define NUFHT_W_DISPATCH(FN, T, Wv, ...)          \
+  switch (Wv) {                                   \
+    case 2: rc = FN<T, 2>(__VA_ARGS__); break;    \
+    case 3: rc = FN<T, 3>(__VA_ARGS__); break;    \
+    case 4: rc = FN<T, 4>(__VA_ARGS__); break;    \
+    case 5: rc = FN<T, 5>(__VA_ARGS__); break;    \
+    case 6: rc = FN<T, 6>(__VA_ARGS__); break;    \
+    case 7: rc = FN<T, 7>(__VA_ARGS__); break;    \
+    case 8: rc = FN<T, 8>(__VA_ARGS__); break;    \
+    case 9: rc = FN<T, 9>(__VA_ARGS__); break;    \
+    case 10: rc = FN<T, 10>(__VA_ARGS__); break;  \
+    case 11: rc = FN<T, 11>(__VA_ARGS__); break;  \
+    case 12: rc = FN<T, 12>(__VA_ARGS__); break;  \
+    case 13: rc = FN<T, 13>(__VA_ARGS__); break;  \
+    case 14: rc = FN<T, 14>(__VA_ARGS__); break;  \
+    case 15: rc = FN<T, 15>(__VA_ARGS__); break;  \
+    default: rc = FN<T, 16>(__VA_ARGS__); break;  \
   }
 
-int run_asy(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
-            double sgn) {
+template <typename T>
+int run_asy_t(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
+              double sgn) {
+  using C2 = typename Cplx<T>::type;
   int rc = 0;
   const size_t V = (size_t)D.NLP * B;
+  C2* grid = static_cast<C2*>(D.d_grid);
   {
     PhaseScope ps(kPhaseSpread, st);
     if (D.chunk_cell_end > D.chunk_cell_begin)
-      NUFHT_CUDA_TRY(cudaMemsetAsync(D.d_grid + (size_t)D.chunk_cell_begin * V, 0,
-                                     sizeof(double2) * (size_t)(D.chunk_cell_end - D.chunk_cell_begin) * V, st));
+      NUFHT_CUDA_TRY(cudaMemsetAsync(grid + (size_t)D.chunk_cell_begin * V, 0,
+                                     sizeof(C2) * (size_t)(D.chunk_cell_end - D.chunk_cell_begin) * V, st));
     for (const AsyClass& K : D.classes) {
-      if (K.nspread == 0) continue;
-      NUFHT_W_DISPATCH(launch_spread, K.W, D, K, cs, ld_cs, B, st);
+      if (K.nspread + K.nspreadA == 0) continue;
+      NUFHT_W_DISPATCH(launch_spread, T, K.W, D, K, cs, ld_cs, B, st);
       if (rc) return rc;
     }
   }
@@ -614,20 +635,30 @@ int run_asy(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, i
     PhaseScope ps(kPhaseFft, st);
     for (const FftGroup& gr : D.groups) {
       cufftSetStream(gr.plan, st);
-      double2* p = D.d_grid + (size_t)gr.cell_off * V;
-      if (cufftExecZ2Z(gr.plan, (cufftDoubleComplex*)p, (cufftDoubleComplex*)p, CUFFT_INVERSE) != CUFFT_SUCCESS)
-        return NUFHT_E_CUDA;
+      C2* p = grid + (size_t)gr.cell_off * V;
+      cufftResult fr;
+      if (sizeof(T) == 8)
+        fr = cufftExecZ2Z(gr.plan, (cufftDoubleComplex*)p, (cufftDoubleComplex*)p, CUFFT_INVERSE);
+      else
+        fr = cufftExecC2C(gr.plan, (cufftComplex*)p, (cufftComplex*)p, CUFFT_INVERSE);
+      if (fr != CUFFT_SUCCESS) return NUFHT_E_CUDA;
     }
   }
   {
     PhaseScope ps(kPhaseInterp, st);
     for (const AsyClass& K : D.classes) {
       if (K.ninterp == 0) continue;
-      NUFHT_W_DISPATCH(launch_interp, K.W, D, K, gs, ld_gs, B, st, sgn);
+      NUFHT_W_DISPATCH(launch_interp, T, K.W, D, K, gs, ld_gs, B, st, sgn);
       if (rc) return rc;
     }
   }
   return 0;
+}
+
+int run_asy(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
+            double sgn) {
+  return D.mixed_asy ? run_asy_t<float>(D, cs, ld_cs, gs, ld_gs, B, st, sgn)
+                     : run_asy_t<double>(D, cs, ld_cs, gs, ld_gs, B, st, sgn);
 }
 
 template <int BT>

@@ -33,6 +33,9 @@ struct DirItem { int i0, ni, j0, nj, lanes; };
 struct AsyBoxD {
   int i0, i1, j0, j1;
   double C, D, h;
+  double rref;          // smallest source radius of the box: the source factors are
+                        // (rref/r)^(lp+1/2) <= 1 and the target factors (k rref)^-(lp+1/2)
+                        // <= z_split^-(lp+1/2), so both stay in single-precision range
   int half, n2;
   int mode;             // 0: CTAs own grid tiles; 1: CTAs own source chunks (dense boxes)
   int cls;              // kernel class (oversampling and kernel width)
@@ -70,7 +73,9 @@ struct AsyClass {
   double sigma;
   int W;
   AsyConst ac;
-  int spread0, nspread, interp0, ninterp;
+  int spread0, nspread;    // windowed spreading items (modes 0 and 2)
+  int spreadA0, nspreadA;  // atomic spreading items (mode 1)
+  int interp0, ninterp;
 };
 
 int spread_width_for_tol(double tol);
@@ -122,7 +127,8 @@ struct DevicePlan {
   int fft_B = 0;             // batch size the FFT plans were made for
   size_t fft_work_bytes = 0;
   size_t ws_bytes = 0;
-  double2* d_grid = nullptr;
+  void* d_grid = nullptr;    // complex FP64 (double2) or, in mixed precision, FP32 (float2)
+  bool mixed_asy = false;    // asymptotic boxes in FP32 (set for NUFHT_B200_MIXED, tol >= 1e-9)
   double* d_partial = nullptr;
   double* d_cheb = nullptr;
   void* d_fft_work = nullptr;
