@@ -69,34 +69,39 @@ __device__ inline void bessel_j01_large(double x, double* J0, double* J1) {
 
 constexpr double kHankelMinX = 17.0;
 
-// J_0(x) and J_1(x) for 0 <= x < 17 from the piecewise Chebyshev expansions of
-// bessel_j01_table.h (unit intervals, Clenshaw summation; error below 2e-16).
-__device__ inline void bessel_j01_small(double x, double* J0, double* J1) {
+// J_0(x) and, when need_j1, J_1(x) for 0 <= x < 17 from the piecewise Chebyshev
+// expansions of bessel_j01_table.h (unit intervals, Clenshaw summation; error below 2e-16).
+__device__ inline void bessel_j01_small(double x, double* J0, double* J1, bool need_j1 = true) {
   int a = (int)x;
   a = a < 0 ? 0 : (a > kJ01Intervals - 1 ? kJ01Intervals - 1 : a);
   const double t = 2.0 * (x - (double)a) - 1.0, t2 = 2.0 * t;
   const double* c0 = kJ01Cheb[0][a];
-  const double* c1 = kJ01Cheb[1][a];
-  double b1 = 0.0, b2 = 0.0, d1 = 0.0, d2 = 0.0;
+  double b1 = 0.0, b2 = 0.0;
 #pragma unroll
   for (int k = kJ01Coefs - 1; k > 0; --k) {
     double bn = fma(t2, b1, c0[k] - b2);
-    double dn = fma(t2, d1, c1[k] - d2);
     b2 = b1;
     b1 = bn;
+  }
+  *J0 = fma(t, b1, c0[0] - b2);
+  if (!need_j1) return;
+  const double* c1 = kJ01Cheb[1][a];
+  double d1 = 0.0, d2 = 0.0;
+#pragma unroll
+  for (int k = kJ01Coefs - 1; k > 0; --k) {
+    double dn = fma(t2, d1, c1[k] - d2);
     d2 = d1;
     d1 = dn;
   }
-  *J0 = fma(t, b1, c0[0] - b2);
   *J1 = fma(t, d1, c1[0] - d2);
 }
 
 __device__ inline double bessel_jn(int n, double x) {
-  double a, b;
+  double a = 0.0, b = 0.0;
   if (x >= kHankelMinX) {
     bessel_j01_large(x, &a, &b);
   } else if (n <= 1 || x > (double)n) {
-    bessel_j01_small(x, &a, &b);
+    bessel_j01_small(x, &a, &b, n != 0);
   }
   if (n == 0) return a;
   if (n == 1) return b;

@@ -214,7 +214,9 @@ void DevicePlan::build_lists() {
     int ni = hb.i1 - hb.i0 + 1;
     int lanes = ni >= kDirThreads ? 1 : std::min(32, kDirThreads / next_pow2(ni));
     int tpc = kDirThreads / lanes;  // targets per CTA
-    int spi = kDirSources * lanes;  // sources per item
+    // The same number of sources per item for every shape: thin boxes (few targets, many
+    // sources) split into many CTAs instead of a few long-running ones.
+    int spi = kDirSources;
     for (int i = hb.i0; i <= hb.i1; i += tpc)
       for (int j = hb.j0; j <= hb.j1; j += spi)
         dir.push_back({i, std::min(tpc, hb.i1 - i + 1), j, std::min(spi, hb.j1 - j + 1), lanes});

@@ -10,7 +10,7 @@
 namespace hankel {
 
 constexpr int kDirThreads = 128;
-constexpr int kDirSources = 1024;  // sources per work item for lanes == 1
+constexpr int kDirSources = 1024;  // sources per work item
 constexpr int kDirChunk = 64;      // sources staged in shared memory per round
 
 template <int BT>
