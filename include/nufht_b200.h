@@ -178,7 +178,7 @@ typedef struct {
     long n_loc, n_asy, n_dir;      /* box counts */
     long fft_points;               /* sum over asymptotic boxes of the FFT length */
     int spread_width;              /* exponential-of-semicircle kernel width */
-    int path;                      /* 0 boxes, 1 all-direct, 2 all-asymptotic (half-integer) */
+    int path;                      /* 0 boxes, 1 all-direct, 2 half-integer order */
     size_t workspace_bytes;        /* device workspace for the last batch size executed */
     int mixed;                     /* 1 when the asymptotic boxes run in FP32 */
 } NufhtB200Info;
@@ -244,6 +244,35 @@ int nufht_b200_fp64_peak(double *tflops);
 int nufht_b200_add_loc_batch_noalloc(double *gs, double nu, const double *rs, const double *cs,
                                      const double *ws, int m, int n, int K, int batch, int ld_cs,
                                      int ld_gs, void *stream);
+
+/* No counterpart in the reference (one problem per call there).  Many independent
+ * transforms -- each a device plan with its own order, grids, tolerance and batch width --
+ * executed by ONE CUDA-graph launch.  Items that share a plan run one after another; other
+ * items run concurrently on up to `branches` parallel branches of the graph, dealt by
+ * estimated work.  branches = 0 tunes the count at creation (1, 2, 4, ... 32) by timing the
+ * graph on the items' own buffers.  cs / gs are DEVICE pointers, fixed for the life of the
+ * batch (the graph records them); g is overwritten.  Creation runs every item once and
+ * sizes all workspaces, so a launch allocates nothing.  The plans must not be executed
+ * elsewhere while a launch of the batch is in flight. */
+typedef struct NufhtB200Batch NufhtB200Batch;
+typedef struct {
+    NufhtDevicePlan *plan;
+    const double *cs;  /* m x batch, leading dimension ld_cs >= m */
+    int ld_cs;
+    double *gs;        /* n x batch, leading dimension ld_gs >= n */
+    int ld_gs;
+    int batch;
+} NufhtB200BatchItem;
+
+int nufht_b200_batch_create(NufhtB200Batch **out, const NufhtB200BatchItem *items, int count,
+                            int branches);
+/* One graph launch on `stream` (a cudaStream_t; asynchronous). */
+int nufht_b200_batch_launch(NufhtB200Batch *batch, void *stream);
+/* Branch count in use, the tuned graph time (ms, 0 when branches was given) and the
+ * number of kernel nodes of the graph. */
+int nufht_b200_batch_info(const NufhtB200Batch *batch, int *branches, float *tuned_ms,
+                          long *kernel_nodes);
+void nufht_b200_batch_destroy(NufhtB200Batch *batch);
 
 /* Where the planning tables were read from (a cache file path), or "generated". */
 const char *nufht_b200_table_source(void);

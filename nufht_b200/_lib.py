@@ -65,6 +65,11 @@ NUFHT_E_NO_DEVICE = -422
 NUFHT_E_TOO_LARGE = -423
 NUFHT_E_BAD_FLAGS = -424
 
+class NufhtB200BatchItem(ctypes.Structure):
+    _fields_ = [("plan", ctypes.c_void_p), ("cs", ctypes.c_void_p), ("ld_cs", ctypes.c_int),
+                ("gs", ctypes.c_void_p), ("ld_gs", ctypes.c_int), ("batch", ctypes.c_int)]
+
+
 _lib = None
 
 
@@ -117,6 +122,12 @@ def _declare(lib):
                                                             ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                             ctypes.c_int, vp]),
         "nufht_b200_phase_times": (ctypes.c_int, [c_double_p, ctypes.c_int]),
+        "nufht_b200_batch_create": (ctypes.c_int, [ctypes.POINTER(vp), ctypes.POINTER(NufhtB200BatchItem),
+                                                   ctypes.c_int, ctypes.c_int]),
+        "nufht_b200_batch_launch": (ctypes.c_int, [vp, vp]),
+        "nufht_b200_batch_info": (ctypes.c_int, [vp, c_int_p, ctypes.POINTER(ctypes.c_float),
+                                                 ctypes.POINTER(ctypes.c_long)]),
+        "nufht_b200_batch_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -1,0 +1,11 @@
+// Asymptotic boxes in single-precision (mixed) arithmetic.
+#include "asy_launch.cuh"
+
+namespace hankel {
+
+int run_asy_f32(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
+              double sgn) {
+  return run_asy_t<float>(D, cs, ld_cs, gs, ld_gs, B, st, sgn);
+}
+
+}  // namespace hankel

@@ -1,0 +1,159 @@
+// Launchers of the asymptotic-box kernels (spread, FFT, interpolation) for one arithmetic
+// type; included by asy_f32.cu and asy_f64.cu, one instantiation each, so that the two
+// precisions compile in parallel.
+#pragma once
+
+#include <cufft.h>
+
+#include <algorithm>
+
+#include "executor.h"
+#include "kernels_asy.cuh"
+
+namespace hankel {
+namespace {
+
+AsyShape asy_shape(const DevicePlan& D, int B, int LPT) {
+  AsyShape L;
+  L.LPT = LPT;
+  L.NG = D.NLP / LPT;
+  int cap = std::max(1, std::min(256 / L.NG, 32));
+  L.BT = std::min(cap, B);
+  L.threads = L.BT * L.NG;
+  L.V_total = D.NLP * B;
+  L.ngy = (B + L.BT - 1) / L.BT;
+  return L;
+}
+
+template <typename T, int W, int LPT, bool WINDOWED>
+int launch_spread_kind(DevicePlan& D, const AsyClass& K, int item0, int nitems, const double* cs, int ld_cs,
+                       int B, cudaStream_t st) {
+  if (nitems == 0) return 0;
+  const AsyShape L = asy_shape(D, B, LPT);
+  size_t sm = spread_smem<T>(W, L.BT * D.NLP, L.NG, L.BT, WINDOWED).total;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_asy_spread<T, W, LPT, WINDOWED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         220 * 1024);
+    attr_set = true;
+  }
+  dim3 g((unsigned)nitems, (unsigned)L.ngy);
+  k_asy_spread<T, W, LPT, WINDOWED><<<g, L.threads, sm, st>>>(
+      D.d_rs, cs, ld_cs, B, (typename Cplx<T>::type*)D.d_grid, D.d_asyb, D.d_spread + item0, D.d_corr, K.ac,
+      L.BT, L.V_total);
+  NUFHT_LAUNCH_CHECK();
+  return 0;
+}
+
+template <typename T, int W, int LPT>
+int launch_spread_lpt(DevicePlan& D, const AsyClass& K, const double* cs, int ld_cs, int B, cudaStream_t st) {
+  int rc = launch_spread_kind<T, W, LPT, true>(D, K, K.spread0, K.nspread, cs, ld_cs, B, st);
+  if (rc) return rc;
+  return launch_spread_kind<T, W, LPT, false>(D, K, K.spreadA0, K.nspreadA, cs, ld_cs, B, st);
+}
+
+template <typename T, int W, int LPT, bool SHFL>
+int launch_interp_lpt(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, int B, cudaStream_t st,
+                      double sgn) {
+  const AsyShape L = asy_shape(D, B, LPT);
+  size_t sm = interp_smem<T>(W, D.NLP, SHFL ? 0 : L.threads).total;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_asy_interp<T, W, LPT, SHFL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         220 * 1024);
+    attr_set = true;
+  }
+  dim3 g((unsigned)K.ninterp, (unsigned)L.ngy);
+  k_asy_interp<T, W, LPT, SHFL><<<g, L.threads, sm, st>>>(
+      D.d_ws, gs, ld_gs, B, (const typename Cplx<T>::type*)D.d_grid, D.d_asyb, D.d_interp + K.interp0,
+      D.d_post, K.ac, L.BT, L.V_total, sgn);
+  NUFHT_LAUNCH_CHECK();
+  return 0;
+}
+
+// Terms per thread (register blocking): LPT = 2, or 1 in double precision for windows wider
+// than 10 (register budget); NLP = 2 (K + 1) is even.  Interpolation reduces a column's
+// partial sums with warp shuffles when its NLP / LPT threads are a power of two.
+template <typename T, int W>
+int launch_spread(DevicePlan& D, const AsyClass& K, const double* cs, int ld_cs, int B, cudaStream_t st) {
+  if constexpr (sizeof(T) == 8 && W > 10) return launch_spread_lpt<T, W, 1>(D, K, cs, ld_cs, B, st);
+  else return launch_spread_lpt<T, W, 2>(D, K, cs, ld_cs, B, st);
+}
+
+template <typename T, int W, int LPT>
+int launch_interp_ng(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, int B, cudaStream_t st, double sgn) {
+  const int NG = D.NLP / LPT;
+  if ((NG & (NG - 1)) == 0) return launch_interp_lpt<T, W, LPT, true>(D, K, gs, ld_gs, B, st, sgn);
+  return launch_interp_lpt<T, W, LPT, false>(D, K, gs, ld_gs, B, st, sgn);
+}
+
+template <typename T, int W>
+int launch_interp(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, int B, cudaStream_t st, double sgn) {
+  if (K.ninterp == 0) return 0;
+  if constexpr (sizeof(T) == 8 && W > 10) return launch_interp_ng<T, W, 1>(D, K, gs, ld_gs, B, st, sgn);
+  else return launch_interp_ng<T, W, 2>(D, K, gs, ld_gs, B, st, sgn);
+}
+
+#define NUFHT_W_DISPATCH(FN, T, Wv, ...)          \
+  switch (Wv) {                                   \
+    case 2: rc = FN<T, 2>(__VA_ARGS__); break;    \
+    case 3: rc = FN<T, 3>(__VA_ARGS__); break;    \
+    case 4: rc = FN<T, 4>(__VA_ARGS__); break;    \
+    case 5: rc = FN<T, 5>(__VA_ARGS__); break;    \
+    case 6: rc = FN<T, 6>(__VA_ARGS__); break;    \
+    case 7: rc = FN<T, 7>(__VA_ARGS__); break;    \
+    case 8: rc = FN<T, 8>(__VA_ARGS__); break;    \
+    case 9: rc = FN<T, 9>(__VA_ARGS__); break;    \
+    case 10: rc = FN<T, 10>(__VA_ARGS__); break;  \
+    case 11: rc = FN<T, 11>(__VA_ARGS__); break;  \
+    case 12: rc = FN<T, 12>(__VA_ARGS__); break;  \
+    case 13: rc = FN<T, 13>(__VA_ARGS__); break;  \
+    case 14: rc = FN<T, 14>(__VA_ARGS__); break;  \
+    case 15: rc = FN<T, 15>(__VA_ARGS__); break;  \
+    default: rc = FN<T, 16>(__VA_ARGS__); break;  \
+  }
+
+template <typename T>
+int run_asy_t(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
+              double sgn) {
+  using C2 = typename Cplx<T>::type;
+  int rc = 0;
+  const size_t V = (size_t)D.NLP * B;
+  C2* grid = static_cast<C2*>(D.d_grid);
+  {
+    PhaseScope ps(kPhaseSpread, st);
+    if (D.chunk_cell_end > D.chunk_cell_begin)
+      NUFHT_CUDA_TRY(cudaMemsetAsync(grid + (size_t)D.chunk_cell_begin * V, 0,
+                                     sizeof(C2) * (size_t)(D.chunk_cell_end - D.chunk_cell_begin) * V, st));
+    for (const AsyClass& K : D.classes) {
+      if (K.nspread + K.nspreadA == 0) continue;
+      NUFHT_W_DISPATCH(launch_spread, T, K.W, D, K, cs, ld_cs, B, st);
+      if (rc) return rc;
+    }
+  }
+  {
+    PhaseScope ps(kPhaseFft, st);
+    for (const FftGroup& gr : D.groups) {
+      cufftSetStream(gr.plan, st);
+      C2* p = grid + (size_t)gr.cell_off * V;
+      cufftResult fr;
+      if (sizeof(T) == 8)
+        fr = cufftExecZ2Z(gr.plan, (cufftDoubleComplex*)p, (cufftDoubleComplex*)p, CUFFT_INVERSE);
+      else
+        fr = cufftExecC2C(gr.plan, (cufftComplex*)p, (cufftComplex*)p, CUFFT_INVERSE);
+      if (fr != CUFFT_SUCCESS) return NUFHT_E_CUDA;
+    }
+  }
+  {
+    PhaseScope ps(kPhaseInterp, st);
+    for (const AsyClass& K : D.classes) {
+      if (K.ninterp == 0) continue;
+      NUFHT_W_DISPATCH(launch_interp, T, K.W, D, K, gs, ld_gs, B, st, sgn);
+      if (rc) return rc;
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+}  // namespace hankel

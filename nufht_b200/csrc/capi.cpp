@@ -2,6 +2,7 @@
 // backed by the GPU executor, and this library's device-plan extension.
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -11,6 +12,7 @@
 #include <mutex>
 #include <vector>
 
+#include "capi_internal.h"
 #include "executor.h"
 #include "nufht_internal.h"
 
@@ -18,10 +20,6 @@ using hankel::DevicePlan;
 using hankel::HBox;
 using hankel::HBoxes;
 using hankel::PlanParams;
-
-struct NufhtDevicePlan {
-  std::unique_ptr<DevicePlan> dp;
-};
 
 namespace {
 
@@ -71,8 +69,41 @@ BoxVector to_boxvec(const std::vector<HBox>& v) {
   return b;
 }
 
+// Smallest argument x from which the terminating Hankel expansion of J_{n+1/2},
+//   J_{n+1/2}(x) = sqrt(2/(pi x)) (cos chi sum_{k even} (-1)^{k/2} a_k x^-k
+//                                  - sin chi sum_{k odd} (-1)^{(k-1)/2} a_k x^-k),
+//   a_k = prod_{i=1..k} (4 nu^2 - (2i-1)^2) / (k! 8^k),  a_k = 0 for k > n,
+// is evaluated without cancellation: there the terms sum to at most kHalfTermSum in
+// magnitude, so the asymptotic boxes' per-term tolerance is amplified at most that much (the
+// integer-order boxes of the planner work at similar term sums, about 10 at z_split).  0 for
+// nu = 1/2, whose expansion is the single term sin(x).
+constexpr double kHalfTermSum = 8.0;
+double half_integer_split(double anu) {
+  const int n = (int)std::llround(anu - 0.5);
+  if (n <= 0) return 0.0;
+  std::vector<double> a(n + 1);
+  a[0] = 1.0;
+  for (int k = 1; k <= n; ++k) a[k] = a[k - 1] * (4.0 * anu * anu - (2.0 * k - 1) * (2.0 * k - 1)) / (8.0 * k);
+  auto sum = [&](double x) {
+    double s = 0.0, p = 1.0;
+    for (int k = 0; k <= n; ++k, p /= x) s += std::fabs(a[k]) * p;
+    return s;
+  };
+  double lo = 1e-6, hi = 1e6;
+  for (int it = 0; it < 200 && hi - lo > 1e-12 * hi; ++it) {
+    double mid = std::sqrt(lo * hi);
+    if (sum(mid) > kHalfTermSum) lo = mid;
+    else hi = mid;
+  }
+  return hi;
+}
+
 // Decide which evaluation path nufht_batch takes (src/fast_hankel_nufht.c:1018-1080) and
-// fill the boxes the executor evaluates.
+// fill the boxes the executor evaluates.  Half-integer orders: the reference evaluates the
+// whole rectangle with the terminating expansion (:1052-1078), which cancels
+// catastrophically at small k r for nu >= 3/2; here pairs with k r below
+// half_integer_split(nu) are summed directly (the planner's partition at that z, local
+// boxes included) and only the rest is asymptotic.
 void choose_path(DevicePlan* D, int min_dim_prod) {
   long long dp = (long long)D->m * (long long)D->n;
   D->loc_boxes.clear();
@@ -84,7 +115,16 @@ void choose_path(DevicePlan* D, int min_dim_prod) {
     D->dir_boxes.push_back(whole);
   } else if (!hankel::is_integer(D->P.nu)) {
     D->path = 2;
-    D->asy_boxes.push_back(whole);
+    const double zh = half_integer_split(std::fabs(D->P.nu));
+    if (zh <= 0.0) {
+      D->asy_boxes.push_back(whole);
+    } else {
+      hankel::HBoxes hb;
+      hankel::make_boxes(D->h_rs.data(), D->m, D->h_ws.data(), D->n, zh, 0, min_dim_prod, INT_MAX, &hb);
+      D->asy_boxes = hb.asy;
+      D->dir_boxes = hb.dir;
+      D->dir_boxes.insert(D->dir_boxes.end(), hb.loc.begin(), hb.loc.end());
+    }
   } else {
     D->path = 0;
     if (D->P.K_loc >= 0) D->loc_boxes = D->plan_loc;

@@ -44,23 +44,14 @@ struct PhaseMark {
 };
 std::vector<PhaseMark> g_phase_marks;
 
-struct PhaseScope {
-  PhaseMark mk{-1, nullptr, nullptr};
-  cudaStream_t st;
-  PhaseScope(int phase, cudaStream_t s) : st(s) {
-    if (!g_phase_timing.load(std::memory_order_relaxed)) return;
-    mk.phase = phase;
-    cudaEventCreate(&mk.a);
-    cudaEventCreate(&mk.b);
-    cudaEventRecord(mk.a, st);
-  }
-  ~PhaseScope() {
-    if (mk.phase < 0) return;
-    cudaEventRecord(mk.b, st);
-    std::lock_guard<std::mutex> lk(g_phase_mu);
-    g_phase_marks.push_back(mk);
-  }
-};
+}  // namespace
+
+void phase_record(int phase, cudaEvent_t a, cudaEvent_t b) {
+  std::lock_guard<std::mutex> lk(g_phase_mu);
+  g_phase_marks.push_back({phase, a, b});
+}
+
+namespace {
 
 template <typename T>
 int upload(const std::vector<T>& h, T** d) {
@@ -533,134 +524,10 @@ int DevicePlan::ensure_workspace(int B) {
 
 namespace {
 
-struct AsyLaunch {
-  int BTH, BT, VCTA, V_total, ngy;
-};
-
-// CTA shape with VPT vectors per thread: BTH column slots (NLP * BTH threads, at most
-// 256), BT = VPT * BTH columns per CTA.
-AsyLaunch asy_launch_shape(const DevicePlan& D, int B, int VPT) {
-  AsyLaunch L;
-  int cap = std::max(1, std::min(256 / D.NLP, 32));
-  L.BTH = std::min(cap, (B + VPT - 1) / VPT);
-  L.BT = L.BTH * VPT;
-  L.VCTA = D.NLP * L.BTH;
-  L.V_total = D.NLP * B;
-  L.ngy = (B + L.BT - 1) / L.BT;
-  return L;
-}
-
-template <typename T, int W, bool WINDOWED>
-int launch_spread_kind(DevicePlan& D, const AsyClass& K, int item0, int nitems, const double* cs, int ld_cs,
-                       int B, cudaStream_t st) {
-  if (nitems == 0) return 0;
-  const AsyLaunch L = asy_launch_shape(D, B, 1);
-  size_t sm = spread_smem<T>(W, L.VCTA, D.NLP, L.BT, WINDOWED).total;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_asy_spread<T, W, WINDOWED>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    attr_set = true;
-  }
-  dim3 g((unsigned)nitems, (unsigned)L.ngy);
-  k_asy_spread<T, W, WINDOWED><<<g, L.VCTA, sm, st>>>(D.d_rs, cs, ld_cs, B, (typename Cplx<T>::type*)D.d_grid,
-                                                      D.d_asyb, D.d_spread + item0, D.d_corr, K.ac, L.BT,
-                                                      L.V_total);
-  NUFHT_LAUNCH_CHECK();
-  return 0;
-}
-
-template <typename T, int W>
-int launch_spread(DevicePlan& D, const AsyClass& K, const double* cs, int ld_cs, int B, cudaStream_t st) {
-  int rc = launch_spread_kind<T, W, true>(D, K, K.spread0, K.nspread, cs, ld_cs, B, st);
-  if (rc) return rc;
-  return launch_spread_kind<T, W, false>(D, K, K.spreadA0, K.nspreadA, cs, ld_cs, B, st);
-}
-
-template <typename T, int W>
-int launch_interp(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, int B, cudaStream_t st, double sgn) {
-  if (K.ninterp == 0) return 0;
-  constexpr int VPT = interp_vpt(W);
-  const AsyLaunch L = asy_launch_shape(D, B, VPT);
-  size_t sm = sizeof(double2) * kInterpChunk * D.NLP + sizeof(double) * kInterpChunk * (L.VCTA * VPT + 1) +
-              sizeof(T) * kInterpChunk * W + sizeof(int) * kInterpChunk;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_asy_interp<T, W, VPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    attr_set = true;
-  }
-  dim3 g((unsigned)K.ninterp, (unsigned)L.ngy);
-  k_asy_interp<T, W, VPT><<<g, L.VCTA, sm, st>>>(D.d_ws, gs, ld_gs, B, (const typename Cplx<T>::type*)D.d_grid,
-                                                 D.d_asyb, D.d_interp + K.interp0, D.d_post, K.ac, L.BTH,
-                                                 L.V_total, sgn);
-  NUFHT_LAUNCH_CHECK();
-  return 0;
-}
-
-#define NUFHT_W_DISPATCH(FN, T, Wv, ...)          \
-  switch (Wv) {                                   \
-    case 2: rc = FN<T, 2>(__VA_ARGS__); break;    \
-    case 3: rc = FN<T, 3>(__VA_ARGS__); break;    \
-    case 4: rc = FN<T, 4>(__VA_ARGS__); break;    \
-    case 5: rc = FN<T, 5>(__VA_ARGS__); break;    \
-    case 6: rc = FN<T, 6>(__VA_ARGS__); break;    \
-    case 7: rc = FN<T, 7>(__VA_ARGS__); break;    \
-    case 8: rc = FN<T, 8>(__VA_ARGS__); break;    \
-    case 9: rc = FN<T, 9>(__VA_ARGS__); break;    \
-    case 10: rc = FN<T, 10>(__VA_ARGS__); break;  \
-    case 11: rc = FN<T, 11>(__VA_ARGS__); break;  \
-    case 12: rc = FN<T, 12>(__VA_ARGS__); break;  \
-    case 13: rc = FN<T, 13>(__VA_ARGS__); break;  \
-    case 14: rc = FN<T, 14>(__VA_ARGS__); break;  \
-    case 15: rc = FN<T, 15>(__VA_ARGS__); break;  \
-    default: rc = FN<T, 16>(__VA_ARGS__); break;  \
-  }
-
-template <typename T>
-int run_asy_t(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
-              double sgn) {
-  using C2 = typename Cplx<T>::type;
-  int rc = 0;
-  const size_t V = (size_t)D.NLP * B;
-  C2* grid = static_cast<C2*>(D.d_grid);
-  {
-    PhaseScope ps(kPhaseSpread, st);
-    if (D.chunk_cell_end > D.chunk_cell_begin)
-      NUFHT_CUDA_TRY(cudaMemsetAsync(grid + (size_t)D.chunk_cell_begin * V, 0,
-                                     sizeof(C2) * (size_t)(D.chunk_cell_end - D.chunk_cell_begin) * V, st));
-    for (const AsyClass& K : D.classes) {
-      if (K.nspread + K.nspreadA == 0) continue;
-      NUFHT_W_DISPATCH(launch_spread, T, K.W, D, K, cs, ld_cs, B, st);
-      if (rc) return rc;
-    }
-  }
-  {
-    PhaseScope ps(kPhaseFft, st);
-    for (const FftGroup& gr : D.groups) {
-      cufftSetStream(gr.plan, st);
-      C2* p = grid + (size_t)gr.cell_off * V;
-      cufftResult fr;
-      if (sizeof(T) == 8)
-        fr = cufftExecZ2Z(gr.plan, (cufftDoubleComplex*)p, (cufftDoubleComplex*)p, CUFFT_INVERSE);
-      else
-        fr = cufftExecC2C(gr.plan, (cufftComplex*)p, (cufftComplex*)p, CUFFT_INVERSE);
-      if (fr != CUFFT_SUCCESS) return NUFHT_E_CUDA;
-    }
-  }
-  {
-    PhaseScope ps(kPhaseInterp, st);
-    for (const AsyClass& K : D.classes) {
-      if (K.ninterp == 0) continue;
-      NUFHT_W_DISPATCH(launch_interp, T, K.W, D, K, gs, ld_gs, B, st, sgn);
-      if (rc) return rc;
-    }
-  }
-  return 0;
-}
-
 int run_asy(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
             double sgn) {
-  return D.mixed_asy ? run_asy_t<float>(D, cs, ld_cs, gs, ld_gs, B, st, sgn)
-                     : run_asy_t<double>(D, cs, ld_cs, gs, ld_gs, B, st, sgn);
+  return D.mixed_asy ? run_asy_f32(D, cs, ld_cs, gs, ld_gs, B, st, sgn)
+                     : run_asy_f64(D, cs, ld_cs, gs, ld_gs, B, st, sgn);
 }
 
 template <int BT>

@@ -158,6 +158,32 @@ extern std::atomic<bool> g_phase_timing;
 enum { kPhaseZero = 0, kPhaseLocProj, kPhaseLocEval, kPhaseSpread, kPhaseFft, kPhaseInterp, kPhaseDir,
        kNumPhases };
 int phase_times(double* ms, int nphase);
+void phase_record(int phase, cudaEvent_t a, cudaEvent_t b);
+
+// Device events around one phase of run(), when phase timing is on.
+struct PhaseScope {
+  int phase = -1;
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t st;
+  PhaseScope(int ph, cudaStream_t s) : st(s) {
+    if (!g_phase_timing.load(std::memory_order_relaxed)) return;
+    phase = ph;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, st);
+  }
+  ~PhaseScope() {
+    if (phase < 0) return;
+    cudaEventRecord(b, st);
+    phase_record(phase, a, b);
+  }
+};
+
+// The asymptotic boxes of one run() in single (mixed) or double precision.
+int run_asy_f32(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
+                double sgn);
+int run_asy_f64(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
+                double sgn);
 
 int run_besselj(double nu, const double* x, double* out, long count, cudaStream_t st);
 

@@ -34,11 +34,6 @@ constexpr int kTileMaxSources = 4096;
 constexpr int kInterpTile = 128;    // targets per interpolation CTA
 constexpr int kInterpChunk = 32;    // targets per shared-memory round
 
-// Window capacity (cells) of a spreading CTA for kernel width W.
-__host__ __device__ constexpr int spread_window(int W) { return W + 8 > kSpreadTile ? W + 8 : kSpreadTile; }
-// Vectors per interpolating thread for kernel width W.
-__host__ __device__ constexpr int interp_vpt(int W) { return W <= 12 ? 2 : 1; }
-
 template <typename T> struct Cplx;
 template <> struct Cplx<double> { using type = double2; };
 template <> struct Cplx<float> { using type = float2; };
@@ -59,30 +54,76 @@ __device__ __forceinline__ float es_kernel_t(float u, float ihw, float beta) {
   return s > 0.0f ? expf(beta * (sqrtf(s) - 1.0f)) : 0.0f;
 }
 
+// Work split of the spreading and interpolation CTAs.  Thread (tl, g) owns LPT
+// consecutive expansion terms lp = g LPT .. g LPT + LPT - 1 of column t0 + tl, so every
+// kernel weight read from shared memory feeds 2 LPT multiply-adds (register blocking), and
+// the LPT source amplitudes (rref / r)^(lp + 1/2) c follow from one staged value by
+// multiplications with rref / r.  NG = NLP / LPT threads per column, BT columns per CTA.
+struct AsyShape {
+  int LPT, NG, BT, threads, ngy, V_total;
+};
+
+// Staged kernel weights per source (complex) and per target (real), padded so that every
+// row is read with 16-byte shared-memory loads.
+template <typename T>
+__host__ __device__ constexpr int spread_we(int W) { return sizeof(T) == 4 ? (W + 1) & ~1 : W; }
+template <typename T>
+__host__ __device__ constexpr int interp_we(int W) { return sizeof(T) == 4 ? (W + 3) & ~3 : (W + 1) & ~1; }
+
+__host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+
 // Shared-memory layout of k_asy_spread (byte offsets, each region 16-byte aligned); the
 // host sizes the launch with the same function.
 struct SpreadSmem {
-  size_t win, wc, ph, u, rho, c, l0, total;
+  size_t win, wc, rq, c, u, ph, l0, end, total;
 };
-__host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 template <typename T>
-__host__ __device__ inline SpreadSmem spread_smem(int W, int VCTA, int NLP, int BT, bool windowed) {
+__host__ __device__ inline SpreadSmem spread_smem(int W, int VCTA, int NG, int BT, bool windowed) {
   SpreadSmem L{};
-  size_t c2 = 2 * sizeof(T);
+  const size_t c2 = 2 * sizeof(T);
   L.win = 0;
-  L.wc = align16(L.win + (windowed ? (size_t)spread_window(W) * (VCTA + 1) * c2 : 0));
-  L.ph = align16(L.wc + (size_t)kSpreadChunk * W * c2);
-  L.u = align16(L.ph + (size_t)kSpreadChunk * 16);
-  L.rho = align16(L.u + (size_t)kSpreadChunk * 8);
-  L.c = align16(L.rho + (size_t)kSpreadChunk * NLP * sizeof(T));
-  L.l0 = align16(L.c + (size_t)BT * (kSpreadChunk + 1) * sizeof(T));
-  L.total = align16(L.l0 + (size_t)kSpreadChunk * 4);
+  L.wc = align16(L.win + (windowed ? (size_t)kSpreadTile * (VCTA + 1) * c2 : 0));
+  L.rq = align16(L.wc + (size_t)kSpreadChunk * spread_we<T>(W) * c2);
+  L.c = align16(L.rq + (size_t)kSpreadChunk * NG * c2);
+  L.u = align16(L.c + (size_t)BT * (kSpreadChunk + 1) * sizeof(T));
+  L.ph = align16(L.u + (size_t)kSpreadChunk * sizeof(double));
+  L.l0 = align16(L.ph + (size_t)kSpreadChunk * c2);
+  L.end = align16(L.l0 + (size_t)kSpreadChunk * 4);
+  L.total = align16(L.end + (size_t)kSpreadChunk * 4);
+  return L;
+}
+
+// Index one past the run of equal values that contains a[s] in the non-decreasing a[0, n).
+__device__ __forceinline__ int run_end(const int* a, int n, int s) {
+  const int v = a[s];
+  int lo = s + 1, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (a[mid] > v) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
+// Shared-memory layout of k_asy_interp.
+struct InterpSmem {
+  size_t mu, y, wt, q0, end, total;
+};
+template <typename T>
+__host__ __device__ inline InterpSmem interp_smem(int W, int NLP, int threads) {
+  InterpSmem L{};
+  L.mu = 0;
+  L.y = align16(L.mu + (size_t)kInterpChunk * NLP * 2 * sizeof(T));
+  L.wt = align16(L.y + (threads > 0 ? (size_t)kInterpChunk * (threads + 1) * sizeof(double) : 0));
+  L.q0 = align16(L.wt + (size_t)kInterpChunk * interp_we<T>(W) * sizeof(T));
+  L.end = align16(L.q0 + (size_t)kInterpChunk * 4);
+  L.total = align16(L.end + (size_t)kInterpChunk * 4);
   return L;
 }
 
 // Plan-time tables: 1/psi-hat(2 pi l / n2) for each box cell l, and
 // exp(i (phi + k C)) / psi-hat((k - D) h) for each box target.
-__global__ void k_asy_setup_cells(const AsyBoxD* __restrict__ boxes, AsyConst P,
+static __global__ void k_asy_setup_cells(const AsyBoxD* __restrict__ boxes, AsyConst P,
                                   double* __restrict__ corr) {
   const AsyBoxD bx = boxes[blockIdx.y];
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < 2 * bx.half + 1; c += gridDim.x * blockDim.x) {
@@ -91,7 +132,7 @@ __global__ void k_asy_setup_cells(const AsyBoxD* __restrict__ boxes, AsyConst P,
   }
 }
 
-__global__ void k_asy_setup_targets(const double* __restrict__ ws, const AsyBoxD* __restrict__ boxes,
+static __global__ void k_asy_setup_targets(const double* __restrict__ ws, const AsyBoxD* __restrict__ boxes,
                                     AsyConst P, double2* __restrict__ post) {
   const AsyBoxD bx = boxes[blockIdx.y];
   const int ni = bx.i1 - bx.i0 + 1;
@@ -105,14 +146,83 @@ __global__ void k_asy_setup_targets(const double* __restrict__ ws, const AsyBoxD
   }
 }
 
-// Stage 1.  Thread (tl, lp) of the CTA owns term lp of column t0 + tl (vector
-// v = t0 * NLP + tid).  Sources are sorted, so those whose kernel support starts at the
-// same cell accumulate in registers; the accumulators go, once per cell change, to a
-// shared window of the CTA's own cells (WINDOWED: mode-0 tiles, written with plain stores
-// at the end) or straight to the pre-zeroed grid with atomic adds (mode-1 source chunks of
-// dense boxes, where cell changes are rare).  The source phase exp(i D x) is folded into
-// complex kernel weights staged once per source.
-template <typename T, int W, bool WINDOWED>
+// Weights of one source or target from shared memory (16-byte loads).
+template <int WE>
+__device__ __forceinline__ void load_weights(const float2* src, float2 (&w)[WE]) {
+  const float4* p = reinterpret_cast<const float4*>(src);
+#pragma unroll
+  for (int q = 0; q < WE / 2; ++q) {
+    float4 v = p[q];
+    w[2 * q] = make_float2(v.x, v.y);
+    w[2 * q + 1] = make_float2(v.z, v.w);
+  }
+}
+template <int WE>
+__device__ __forceinline__ void load_weights(const double2* src, double2 (&w)[WE]) {
+#pragma unroll
+  for (int q = 0; q < WE; ++q) w[q] = src[q];
+}
+template <int WE>
+__device__ __forceinline__ void load_weights(const float* src, float (&w)[WE]) {
+  const float4* p = reinterpret_cast<const float4*>(src);
+#pragma unroll
+  for (int q = 0; q < WE / 4; ++q) {
+    float4 v = p[q];
+    w[4 * q] = v.x;
+    w[4 * q + 1] = v.y;
+    w[4 * q + 2] = v.z;
+    w[4 * q + 3] = v.w;
+  }
+}
+template <int WE>
+__device__ __forceinline__ void load_weights(const double* src, double (&w)[WE]) {
+  const double2* p = reinterpret_cast<const double2*>(src);
+#pragma unroll
+  for (int q = 0; q < WE / 2; ++q) {
+    double2 v = p[q];
+    w[2 * q] = v.x;
+    w[2 * q + 1] = v.y;
+  }
+}
+
+// acc += w * a for complex w and real a: one packed two-lane FMA in single precision
+// (fma.rn.f32x2, sm_100 and later), two FMAs in double.
+__device__ __forceinline__ void cfma(float2& acc, float2 w, float a) {
+  unsigned long long rd;
+  const unsigned long long rw = (unsigned long long)__float_as_uint(w.x) |
+                                ((unsigned long long)__float_as_uint(w.y) << 32);
+  const unsigned long long ra = (unsigned long long)__float_as_uint(a) |
+                                ((unsigned long long)__float_as_uint(a) << 32);
+  const unsigned long long rc = (unsigned long long)__float_as_uint(acc.x) |
+                                ((unsigned long long)__float_as_uint(acc.y) << 32);
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(rd) : "l"(rw), "l"(ra), "l"(rc));
+  acc.x = __uint_as_float((unsigned)(rd & 0xffffffffull));
+  acc.y = __uint_as_float((unsigned)(rd >> 32));
+}
+__device__ __forceinline__ void cfma(double2& acc, double2 w, double a) {
+  acc.x = fma(w.x, a, acc.x);
+  acc.y = fma(w.y, a, acc.y);
+}
+
+__device__ __forceinline__ void grid_atomic_add(float2* p, float2 v) {
+  atomicAdd(p, v);  // one vector reduction (sm_90 and later)
+}
+__device__ __forceinline__ void grid_atomic_add(double2* p, double2 v) {
+  atomicAdd(&p->x, v.x);
+  atomicAdd(&p->y, v.y);
+}
+
+// Stage 1.  Sources are sorted, so the first cell l0 of their kernel support never
+// decreases.  The CTA walks the cells c in order; at cell c it adds every source with
+// l0 == c into W register accumulators per vector, then cell c is final and leaves.  The
+// accumulators form a ring indexed (position + tap) mod W, and the walk is unrolled W times
+// so that every ring index is a compile-time constant: no register moves as the window
+// advances.  A finished cell goes to a shared window of the CTA's own cells (WINDOWED,
+// mode-0 tiles; written to the grid with coalesced stores at the end) or is added
+// atomically to the pre-zeroed grid (mode-1 source chunks of dense boxes).  Empty stretches
+// between sources are skipped once the ring is empty.  The source phase exp(i D x) is folded
+// into complex kernel weights staged once per source.
+template <typename T, int W, int LPT, bool WINDOWED>
 __global__ void __launch_bounds__(256) k_asy_spread(
     const double* __restrict__ rs, const double* __restrict__ cs, int ld_cs, int B,
     typename Cplx<T>::type* __restrict__ grid, const AsyBoxD* __restrict__ boxes,
@@ -120,22 +230,26 @@ __global__ void __launch_bounds__(256) k_asy_spread(
     int V_total) {
   using C2 = typename Cplx<T>::type;
   constexpr int SCP = kSpreadChunk + 1;  // padded row of the staged coefficients
+  constexpr int WE = spread_we<T>(W);
   const SpreadItem it = items[blockIdx.x];
   const AsyBoxD bx = boxes[it.box];
   const int NLP = P.NLP;
-  const int VCTA = blockDim.x;
+  const int NG = NLP / LPT;
+  const int nthr = blockDim.x;
+  const int VCTA = BT * NLP;
   const int WP = VCTA + 1;  // padded window row
   const int tid = threadIdx.x;
-  const int tl = tid / NLP, lp = tid - tl * NLP;
+  const int tl = tid / NG, g = tid - tl * NG;
   const int t0 = blockIdx.y * BT;
   const int v0 = t0 * NLP;
   const int nv = min(VCTA, V_total - v0);  // valid vectors of this CTA
-  const bool active = tid < nv;
+  const int vloc = tl * NLP + g * LPT;     // first of this thread's vectors within the CTA
+  const bool active = tl < BT && t0 + tl < B;
   C2* gbox = grid + (size_t)bx.cell_off * (size_t)V_total;
   const int nc = it.ncell;
 
   if (WINDOWED && it.mode == 2) {  // zero padding of the FFT input: threads along cells
-    for (int e = tid; e < nc * nv; e += VCTA) {
+    for (int e = tid; e < nc * nv; e += nthr) {
       int vv = e / nc, cell = e - vv * nc;
       gbox[(size_t)(v0 + vv) * bx.n2 + it.fft_start + cell] = cmake<T>(0, 0);
     }
@@ -143,58 +257,25 @@ __global__ void __launch_bounds__(256) k_asy_spread(
   }
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const SpreadSmem L = spread_smem<T>(W, VCTA, NLP, BT, WINDOWED);
-  C2* win = reinterpret_cast<C2*>(smem_raw + L.win);       // [WIN][WP]
-  C2* s_wc = reinterpret_cast<C2*>(smem_raw + L.wc);       // [SCH][W]
-  double2* s_ph = reinterpret_cast<double2*>(smem_raw + L.ph);  // [SCH]
-  double* s_u = reinterpret_cast<double*>(smem_raw + L.u);  // [SCH]
-  T* s_rho = reinterpret_cast<T*>(smem_raw + L.rho);        // [SCH][NLP]
+  const SpreadSmem L = spread_smem<T>(W, VCTA, NG, BT, WINDOWED);
+  C2* win = reinterpret_cast<C2*>(smem_raw + L.win);        // [kSpreadTile][WP]
+  C2* s_wc = reinterpret_cast<C2*>(smem_raw + L.wc);        // [SCH][WE]
+  C2* s_rq = reinterpret_cast<C2*>(smem_raw + L.rq);        // [SCH][NG]: (rho of term g LPT, rref / r)
   T* s_c = reinterpret_cast<T*>(smem_raw + L.c);            // [BT][SCP]
+  double* s_u = reinterpret_cast<double*>(smem_raw + L.u);  // [SCH]
+  C2* s_ph = reinterpret_cast<C2*>(smem_raw + L.ph);        // [SCH]: exp(i D x)
   int* s_l0 = reinterpret_cast<int*>(smem_raw + L.l0);      // [SCH]
+  int* s_end = reinterpret_cast<int*>(smem_raw + L.end);    // [SCH]: end of the equal-l0 run
 
   if (WINDOWED)
-    for (int cell = 0; cell < nc; ++cell) win[cell * WP + tid] = cmake<T>(0, 0);
+    for (int e = tid; e < kSpreadTile * WP; e += nthr) win[e] = cmake<T>(0, 0);
   const T ihw = (T)(2.0 / (double)W);
   const T beta = (T)P.beta;
-  C2 acc[W];
-#pragma unroll
-  for (int q = 0; q < W; ++q) acc[q] = cmake<T>(0, 0);
-  int cur = INT_MIN;
 
-  auto flush = [&](int c0) {
-    if (WINDOWED) {
-#pragma unroll
-      for (int q = 0; q < W; ++q) {
-        int cell = c0 + q - it.l_start;
-        if (cell >= 0 && cell < nc) {
-          C2 w2 = win[cell * WP + tid];
-          w2.x += acc[q].x;
-          w2.y += acc[q].y;
-          win[cell * WP + tid] = w2;
-        }
-        acc[q] = cmake<T>(0, 0);
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < W; ++q) {
-        int l = c0 + q;
-        if (active && l >= -bx.half && l <= bx.half && (acc[q].x != (T)0 || acc[q].y != (T)0)) {
-          T c = (T)corr[bx.corr_off + l + bx.half];
-          int idx = l < 0 ? l + bx.n2 : l;
-          T* dst = reinterpret_cast<T*>(gbox + (size_t)(v0 + tid) * bx.n2 + idx);
-          atomicAdd(dst, acc[q].x * c);
-          atomicAdd(dst + 1, acc[q].y * c);
-        }
-        acc[q] = cmake<T>(0, 0);
-      }
-    }
-  };
-
-  for (int s0 = it.js; s0 < it.je; s0 += kSpreadChunk) {
-    const int ns = min(kSpreadChunk, it.je - s0);
-    __syncthreads();  // previous round's staging fully consumed
-    // Per-source quantities, spread over all threads of the CTA.
-    for (int s = tid; s < ns; s += VCTA) {
+  // Stage sources [s0, s0 + ns) (all threads; barriers on both sides).
+  auto stage = [&](int s0, int ns) {
+    __syncthreads();  // previous round fully consumed
+    for (int s = tid; s < ns; s += nthr) {
       double r = rs[s0 + s];
       double x = r - bx.C;
       double u = x / bx.h;
@@ -202,111 +283,195 @@ __global__ void __launch_bounds__(256) k_asy_spread(
       s_l0[s] = (int)ceil(u - 0.5 * W);
       double sn, cn;
       sincos(bx.D * x, &sn, &cn);
-      s_ph[s] = make_double2(cn, sn);
-    }
-    for (int e = tid; e < ns * NLP; e += VCTA) {
-      int s = e / NLP, q = e - s * NLP;
-      double r = rs[s0 + s];
-      double rho = 0.0;
-      if (r > 0.0) {  // (rref / r)^(q + 1/2); sources at r = 0 contribute nothing
-        double ir = bx.rref / r;
-        rho = sqrt(ir);
-        for (int z = 0; z < q; ++z) rho *= ir;
+      s_ph[s] = cmake<T>((T)cn, (T)sn);
+      double ir = r > 0.0 ? bx.rref / r : 0.0;  // sources at r = 0 contribute nothing
+      double rho = sqrt(ir);
+      for (int q = 0; q < NG; ++q) {
+        s_rq[s * NG + q] = cmake<T>((T)rho, (T)ir);
+        for (int z = 0; z < LPT; ++z) rho *= ir;
       }
-      s_rho[e] = (T)rho;
     }
-    for (int e = tid; e < ns * BT; e += VCTA) {
+    for (int e = tid; e < ns * BT; e += nthr) {
       int tt = e / ns, s = e - tt * ns;
       s_c[tt * SCP + s] = (T)((t0 + tt < B) ? cs[(size_t)(t0 + tt) * ld_cs + s0 + s] : 0.0);
     }
     __syncthreads();
-    for (int e = tid; e < ns * W; e += VCTA) {
-      int s = e / W, q = e - s * W;
-      T w = es_kernel_t((T)((double)(s_l0[s] + q) - s_u[s]), ihw, beta);
-      double2 ph = s_ph[s];
-      s_wc[e] = cmake<T>(w * (T)ph.x, w * (T)ph.y);
+    for (int e = tid; e < ns * WE; e += nthr) {
+      int s = e / WE, q = e - s * WE;
+      T w = q < W ? es_kernel_t((T)((double)(s_l0[s] + q) - s_u[s]), ihw, beta) : (T)0;
+      C2 ph = s_ph[s];
+      s_wc[e] = cmake<T>(w * ph.x, w * ph.y);
     }
+    for (int s = tid; s < ns; s += nthr) s_end[s] = run_end(s_l0, ns, s);
     __syncthreads();
-    for (int s = 0; s < ns; ++s) {
-      int l0 = s_l0[s];
-      if (l0 != cur) {
-        if (cur != INT_MIN) flush(cur);
-        cur = l0;
-      }
-      T a = s_c[tl * SCP + s] * s_rho[s * NLP + lp];
+  };
+
+  C2 acc[LPT][W];
 #pragma unroll
-      for (int q = 0; q < W; ++q) {
-        C2 wc = s_wc[s * W + q];
-        acc[q].x = fma(wc.x, a, acc[q].x);
-        acc[q].y = fma(wc.y, a, acc[q].y);
+  for (int u = 0; u < LPT; ++u)
+#pragma unroll
+    for (int q = 0; q < W; ++q) acc[u][q] = cmake<T>(0, 0);
+
+  if (it.je > it.js) {
+    int s0 = it.js;
+    int ns = min(kSpreadChunk, it.je - s0);
+    stage(s0, ns);
+    int sp = 0;
+    int c = s_l0[0];
+    // last cell to visit: the last source's support end, or the tile's end
+    int c_end;
+    {
+      double ul = (rs[it.je - 1] - bx.C) / bx.h;
+      c_end = (int)ceil(ul - 0.5 * W) + W - 1;
+      if (WINDOWED) c_end = min(c_end, it.l_start + nc - 1);
+    }
+    int last = INT_MIN / 2;  // cell of the latest source added
+    bool done = c > c_end;
+    while (!done) {
+#pragma unroll
+      for (int jj = 0; jj < W; ++jj) {
+        // sources whose support starts at cell c (ring position jj)
+        for (;;) {
+          if (sp < ns && s_l0[sp] == c) {
+            // the run of sources with l0 == c in this chunk: a known trip count, two
+            // sources per step so that the shared loads of both issue together
+            const int e = s_end[sp];
+            if (tl < BT) {
+              auto add = [&](int s) {
+                const C2 rq = s_rq[s * NG + g];
+                T a = s_c[tl * SCP + s] * rq.x;
+                C2 wc[WE];
+                load_weights<WE>(s_wc + s * WE, wc);
+#pragma unroll
+                for (int u = 0; u < LPT; ++u) {
+#pragma unroll
+                  for (int q = 0; q < W; ++q) cfma(acc[u][(jj + q) % W], wc[q], a);
+                  a *= rq.y;
+                }
+              };
+#pragma unroll 1
+              for (int s = sp; s < e; ++s) add(s);
+            }
+            last = c;
+            sp = e;
+          }
+          if (sp < ns || s0 + ns >= it.je) break;
+          s0 += ns;
+          ns = min(kSpreadChunk, it.je - s0);
+          stage(s0, ns);
+          sp = 0;
+        }
+        // cell c is final
+        if (active) {
+          if (WINDOWED) {
+            const int cl = c - it.l_start;
+            if (cl >= 0 && cl < nc) {
+#pragma unroll
+              for (int u = 0; u < LPT; ++u) win[cl * WP + vloc + u] = acc[u][jj];
+            }
+          } else if (c >= -bx.half && c <= bx.half) {
+            const T cf = (T)corr[bx.corr_off + c + bx.half];
+            const int idx = c < 0 ? c + bx.n2 : c;
+#pragma unroll
+            for (int u = 0; u < LPT; ++u) {
+              const C2 v = acc[u][jj];
+              if (v.x != (T)0 || v.y != (T)0)
+                grid_atomic_add(gbox + (size_t)(v0 + vloc + u) * bx.n2 + idx, cmake<T>(v.x * cf, v.y * cf));
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < LPT; ++u) acc[u][jj] = cmake<T>(0, 0);
+        if (c >= c_end) {
+          done = true;
+          break;
+        }
+        // Past the ring's last non-empty cell the next source's cell can be jumped to: all
+        // accumulators are zero, so any ring position may stand for it.
+        const int nxt = sp < ns ? s_l0[sp] : INT_MAX;
+        if (c >= last + W - 1 && nxt != INT_MAX && nxt > c + 1) c = nxt;
+        else ++c;
       }
     }
   }
-  if (cur != INT_MIN) flush(cur);
   if (!WINDOWED) return;
   __syncthreads();
   // Transposed write-out of the CTA's own cells: consecutive threads take consecutive
   // cells of one vector.
-  for (int e = tid; e < nc * nv; e += VCTA) {
+  for (int e = tid; e < nc * nv; e += nthr) {
     int vv = e / nc, cell = e - vv * nc;
     C2 val = win[cell * WP + vv];
-    T c = (T)corr[bx.corr_off + it.l_start + cell + bx.half];
-    gbox[(size_t)(v0 + vv) * bx.n2 + it.fft_start + cell] = cmake<T>(val.x * c, val.y * c);
+    T cf = (T)corr[bx.corr_off + it.l_start + cell + bx.half];
+    gbox[(size_t)(v0 + vv) * bx.n2 + it.fft_start + cell] = cmake<T>(val.x * cf, val.y * cf);
   }
 }
 
-// Stage 3.  Thread tid owns term lp = tid % NLP of the VPT columns t0 + tid / NLP + u BTH
-// and interpolates them at each target, keeping a sliding window of W grid values per
-// vector in registers; the NLP terms of a column are summed (in FP64) through padded
-// shared memory and added to g.
-template <typename T, int W, int VPT>
+// Stage 3.  Thread (tl, g) owns terms g LPT .. g LPT + LPT - 1 of column t0 + tl.  Targets
+// are sorted, so the first cell q0 of their stencil never decreases; the CTA walks the cells
+// in order with a ring of R = W + 1 grid values per vector in registers: W for the current
+// stencil and one fetched a cell ahead, so that a load has a whole cell step to arrive.  The
+// walk is unrolled R times, which makes every ring index a compile-time constant.  Each
+// thread combines its terms with the per-target factors mu (rounded to the arithmetic type
+// from their FP64 values); the NG partial sums of a column are added with warp shuffles
+// (SHFL: NG a power of two, so a column's threads share a warp) or through shared memory,
+// then atomically into g in FP64.
+template <typename T, int W, int LPT, bool SHFL>
 __global__ void __launch_bounds__(256) k_asy_interp(
     const double* __restrict__ ws, double* __restrict__ gs, int ld_gs, int B,
     const typename Cplx<T>::type* __restrict__ grid, const AsyBoxD* __restrict__ boxes,
-    const InterpItem* __restrict__ items, const double2* __restrict__ post, AsyConst P, int BTH,
+    const InterpItem* __restrict__ items, const double2* __restrict__ post, AsyConst P, int BT,
     int V_total, double sgn) {
   using C2 = typename Cplx<T>::type;
+  constexpr int WE = interp_we<T>(W);
+  constexpr int R = W + 1;
   const InterpItem it = items[blockIdx.x];
   const AsyBoxD bx = boxes[it.box];
   const int NLP = P.NLP;
-  const int VCTA = blockDim.x;
-  const int VV = VCTA * VPT;
-  const int YP = VV + 1;  // padded row of the per-target results
-  const int BT = BTH * VPT;
+  const int NG = NLP / LPT;
+  const int nthr = blockDim.x;
+  const int YP = nthr + 1;  // padded row of the per-target partial sums
   const int tid = threadIdx.x;
-  const int tl = tid / NLP, lp = tid - tl * NLP;
+  const int tl = tid / NG, g = tid - tl * NG;
   const int t0 = blockIdx.y * BT;
-  bool active[VPT];
-#pragma unroll
-  for (int u = 0; u < VPT; ++u) active[u] = t0 + tl + u * BTH < B;
+  const bool active = tl < BT && t0 + tl < B;
+  // lanes of this thread's warp that exist (the block may end inside a warp)
+  const int wbase = tid & ~31;
+  const unsigned wmask = nthr - wbase >= 32 ? 0xffffffffu : ((1u << (nthr - wbase)) - 1u);
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* s_mu = reinterpret_cast<double2*>(smem_raw);          // [KC][NLP]
-  double* s_y = reinterpret_cast<double*>(s_mu + kInterpChunk * NLP);  // [KC][YP]
-  T* s_wt = reinterpret_cast<T*>(s_y + kInterpChunk * YP);       // [KC][W]
-  int* s_q0 = reinterpret_cast<int*>(s_wt + kInterpChunk * W);   // [KC]
+  const InterpSmem L = interp_smem<T>(W, NLP, SHFL ? 0 : nthr);
+  C2* s_mu = reinterpret_cast<C2*>(smem_raw + L.mu);        // [KC][NLP]
+  double* s_y = reinterpret_cast<double*>(smem_raw + L.y);  // [KC][YP] (not SHFL)
+  T* s_wt = reinterpret_cast<T*>(smem_raw + L.wt);          // [KC][WE]
+  int* s_q0 = reinterpret_cast<int*>(smem_raw + L.q0);      // [KC]
+  int* s_end = reinterpret_cast<int*>(smem_raw + L.end);    // [KC]: end of the equal-q0 run
 
   const int n2 = bx.n2;
-  const C2* row[VPT];
+  const C2* row[LPT];
 #pragma unroll
-  for (int u = 0; u < VPT; ++u)
-    row[u] = grid + (size_t)bx.cell_off * (size_t)V_total + (size_t)(t0 * NLP + tid + u * VCTA) * (size_t)n2;
+  for (int u = 0; u < LPT; ++u)
+    row[u] = grid + (size_t)bx.cell_off * (size_t)V_total +
+             (size_t)(active ? (t0 + tl) * NLP + g * LPT + u : 0) * (size_t)n2;
+  double* gcol = gs + (size_t)(active ? t0 + tl : 0) * ld_gs;
   const T ihw = (T)(2.0 / (double)W);
   const T beta = (T)P.beta;
   const double u_scale = bx.h * (double)n2 / (2.0 * M_PI);
-  C2 g[VPT][W];
-  int gq = INT_MIN;
 
-  for (int k0 = it.ks; k0 < it.ke; k0 += kInterpChunk) {
-    const int nk = min(kInterpChunk, it.ke - k0);
-    for (int e = tid; e < nk * W; e += VCTA) {
-      int kk = e / W, q = e - kk * W;
-      double u = (ws[k0 + kk] - bx.D) * u_scale;
-      int q0 = (int)ceil(u - 0.5 * W);
-      if (q == 0) s_q0[kk] = q0;
-      s_wt[kk * W + q] = es_kernel_t((T)(u - (double)(q0 + q)), ihw, beta);
+  auto fetch = [&](int cell, int u) -> C2 {
+    int idx = cell < 0 ? cell + n2 : (cell >= n2 ? cell - n2 : cell);
+    return active ? row[u][idx] : cmake<T>(0, 0);
+  };
+  // Stage targets [k0, k0 + nk) (all threads; barriers on both sides).
+  auto stage = [&](int k0, int nk) {
+    __syncthreads();
+    for (int kk = tid; kk < nk; kk += nthr) {
+      double uu = (ws[k0 + kk] - bx.D) * u_scale;
+      int q0 = (int)ceil(uu - 0.5 * W);
+      s_q0[kk] = q0;
+      for (int q = 0; q < WE; ++q)
+        s_wt[kk * WE + q] = q < W ? es_kernel_t((T)(uu - (double)(q0 + q)), ihw, beta) : (T)0;
     }
-    for (int e = tid; e < nk * NLP; e += VCTA) {
+    for (int e = tid; e < nk * NLP; e += nthr) {
       int kk = e / NLP, q = e - kk * NLP;
       double k = ws[k0 + kk];
       double2 ps = post[bx.post_off + (k0 + kk - bx.i0)];
@@ -316,61 +481,96 @@ __global__ void __launch_bounds__(256) k_asy_interp(
       for (int e2 = 0; e2 < q; ++e2) pw *= ik;
       double sc = P.coef[q] * pw;
       double mr = sc * ps.x, mi = sc * ps.y;
-      s_mu[kk * NLP + q] = (q & 1) ? make_double2(-mi, mr) : make_double2(mr, mi);
+      s_mu[kk * NLP + q] = (q & 1) ? cmake<T>((T)-mi, (T)mr) : cmake<T>((T)mr, (T)mi);
     }
     __syncthreads();
-    for (int kk = 0; kk < nk; ++kk) {
-      int q0 = s_q0[kk];
-      if (q0 != gq) {
-        if (q0 == gq + 1) {
-          int idx = q0 + W - 1;
-          idx = idx < 0 ? idx + n2 : (idx >= n2 ? idx - n2 : idx);
-#pragma unroll
-          for (int u = 0; u < VPT; ++u) {
-#pragma unroll
-            for (int q = 0; q < W - 1; ++q) g[u][q] = g[u][q + 1];
-            g[u][W - 1] = active[u] ? row[u][idx] : cmake<T>(0, 0);
-          }
-        } else {
-#pragma unroll
-          for (int q = 0; q < W; ++q) {
-            int idx = q0 + q;
-            idx = idx < 0 ? idx + n2 : (idx >= n2 ? idx - n2 : idx);
-#pragma unroll
-            for (int u = 0; u < VPT; ++u) g[u][q] = active[u] ? row[u][idx] : cmake<T>(0, 0);
-          }
-        }
-        gq = q0;
-      }
-      T tr[VPT], ti[VPT];
-#pragma unroll
-      for (int u = 0; u < VPT; ++u) tr[u] = ti[u] = (T)0;
-#pragma unroll
-      for (int q = 0; q < W; ++q) {
-        T w = s_wt[kk * W + q];
-#pragma unroll
-        for (int u = 0; u < VPT; ++u) {
-          tr[u] = fma(w, g[u][q].x, tr[u]);
-          ti[u] = fma(w, g[u][q].y, ti[u]);
-        }
-      }
-      double2 mu = s_mu[kk * NLP + lp];
-#pragma unroll
-      for (int u = 0; u < VPT; ++u)
-        s_y[kk * YP + tid + u * VCTA] = mu.x * (double)tr[u] - mu.y * (double)ti[u];
-    }
+    for (int kk = tid; kk < nk; kk += nthr) s_end[kk] = run_end(s_q0, nk, kk);
     __syncthreads();
-    for (int e = tid; e < nk * BT; e += VCTA) {
+  };
+  // Shared-memory reduction of the NG partials of each column (not SHFL; all threads).
+  auto flush = [&](int k0, int nk) {
+    if (SHFL) return;
+    __syncthreads();
+    for (int e = tid; e < nk * BT; e += nthr) {
       int tt = e / nk, kk = e - tt * nk;
       if (t0 + tt < B) {
-        // column tt lives in vectors (tt % BTH) * NLP + q + (tt / BTH) * VCTA
-        const int base = (tt % BTH) * NLP + (tt / BTH) * VCTA;
-        double s = 0.0;
-        for (int q = 0; q < NLP; ++q) s += s_y[kk * YP + base + q];
-        atomicAdd(&gs[(size_t)(t0 + tt) * ld_gs + k0 + kk], sgn * s);
+        double sum = 0.0;
+        for (int q = 0; q < NG; ++q) sum += s_y[kk * YP + tt * NG + q];
+        atomicAdd(&gs[(size_t)(t0 + tt) * ld_gs + k0 + kk], sgn * sum);
       }
     }
-    __syncthreads();
+  };
+
+  if (it.ke <= it.ks) return;
+  int k0 = it.ks;
+  int nk = min(kInterpChunk, it.ke - k0);
+  stage(k0, nk);
+  int kp = 0;
+  int c = s_q0[0];
+  C2 gw[LPT][R];
+#pragma unroll
+  for (int q = 0; q < R; ++q)
+#pragma unroll
+    for (int u = 0; u < LPT; ++u) gw[u][q] = fetch(c + q, u);
+  bool done = false;
+  while (!done) {
+#pragma unroll
+    for (int jj = 0; jj < R; ++jj) {
+      // targets whose stencil starts at cell c (ring position jj)
+      for (;;) {
+        if (kp < nk && s_q0[kp] == c) {
+          const int e = s_end[kp];
+          if (tl < BT) {
+#pragma unroll 1
+            for (int k = kp; k < e; ++k) {
+              T wt[WE];
+              load_weights<WE>(s_wt + k * WE, wt);
+              T y = (T)0;
+#pragma unroll
+              for (int u = 0; u < LPT; ++u) {
+                C2 f = cmake<T>(0, 0);
+#pragma unroll
+                for (int q = 0; q < W; ++q) cfma(f, gw[u][(jj + q) % R], wt[q]);
+                const C2 mu = s_mu[k * NLP + g * LPT + u];
+                y = fma(mu.x, f.x, y);
+                y = fma(-mu.y, f.y, y);
+              }
+              if (SHFL) {
+                for (int off = NG >> 1; off > 0; off >>= 1) y += __shfl_xor_sync(wmask, y, off);
+                if (g == 0 && active) atomicAdd(gcol + k0 + k, sgn * (double)y);
+              } else {
+                s_y[k * YP + tid] = (double)y;
+              }
+            }
+          }
+          kp = e;
+        }
+        if (kp < nk) break;
+        flush(k0, nk);
+        if (k0 + nk >= it.ke) {
+          done = true;
+          break;
+        }
+        k0 += nk;
+        nk = min(kInterpChunk, it.ke - k0);
+        stage(k0, nk);
+        kp = 0;
+      }
+      if (done) break;
+      // advance to the next target's cell; ring position jj + 1 stands for it
+      const int nxt = s_q0[kp];
+      if (nxt == c + 1) {
+        // the slot of cell c takes cell c + R (one cell ahead of the next stencil)
+#pragma unroll
+        for (int u = 0; u < LPT; ++u) gw[u][jj] = fetch(c + R, u);
+      } else {
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+#pragma unroll
+          for (int u = 0; u < LPT; ++u) gw[u][(jj + 1 + q) % R] = fetch(nxt + q, u);
+      }
+      c = nxt;
+    }
   }
 }
 

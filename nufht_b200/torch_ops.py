@@ -112,17 +112,29 @@ def nufht(c, r, k, nu, tol=1e-8, mixed=False, plans=None):
 
 
 class HankelTransform(torch.nn.Module):
-    """Module wrapper: fixed order and tolerance; plans cached for the last grids seen."""
+    """Module wrapper: fixed order and tolerance; plans cached for the last grids seen.
 
-    def __init__(self, nu, tol=1e-8, mixed=False):
+    extended_tables fills the asymptotic table entry the reference leaves empty (K_asy = 10,
+    reached by |nu| >= 35 at tol 1e-8)."""
+
+    def __init__(self, nu, tol=1e-8, mixed=False, extended_tables=False):
         super().__init__()
         self.nu, self.tol, self.mixed = float(nu), float(tol), bool(mixed)
+        self.extended = bool(extended_tables)
         self._plans = None
         self._key = None
 
     def forward(self, c, r, k):
         key = (r.data_ptr(), k.data_ptr(), r.numel(), k.numel(), r._version, k._version)
         if self._plans is None or key != self._key:
-            self._plans = HankelPlans(self.nu, r, k, self.tol, self.mixed)
+            self.release()
+            self._plans = HankelPlans(self.nu, r, k, self.tol, self.mixed, self.extended)
             self._key = key
         return nufht(c, r, k, self.nu, self.tol, self.mixed, plans=self._plans)
+
+    def release(self):
+        """Free the cached plans and their device workspaces."""
+        if self._plans is not None:
+            self._plans.close()
+        self._plans = None
+        self._key = None
