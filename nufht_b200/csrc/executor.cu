@@ -539,15 +539,66 @@ int launch_dir(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs
   return 0;
 }
 
+// Shared-memory budget of the local-expansion kernels (doubles).
+constexpr size_t kLocSmemDoubles = 200 * 1024 / 8;
+
 template <int MAXO>
-int launch_loc_eval(DevicePlan& D, double* gs, int ld_gs, int B, cudaStream_t st, double sgn) {
-  size_t sm = sizeof(double) * D.KL1 * B;
-  if (sm > 48 * 1024)
-    cudaFuncSetAttribute(k_loc_eval<MAXO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_loc_eval<MAXO><<<(unsigned)D.eval.size(), kLocTargets, sm, st>>>(
-      D.d_ws, gs, ld_gs, B, D.d_locb, D.d_eval, D.d_cheb, D.P.K_loc, D.nu2 / 2, sgn);
+int launch_loc_eval_t(const double* ws, double* gs, int ld_gs, int B, const LocBoxD* d_box, const EvalItem* d_eval,
+                      int neval, const double* d_cheb, int K, int nu_int, double sgn, cudaStream_t st) {
+  const int KL1 = K + 1;
+  const int BTC = (int)std::max<size_t>(1, std::min<size_t>((size_t)B, kLocSmemDoubles / (size_t)KL1));
+  const size_t sm = sizeof(double) * (size_t)KL1 * BTC;
+  if (sm > 48 * 1024) cudaFuncSetAttribute(k_loc_eval<MAXO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_loc_eval<MAXO><<<(unsigned)neval, kLocTargets, sm, st>>>(ws, gs, ld_gs, B, d_box, d_eval, d_cheb, K, nu_int,
+                                                            sgn, BTC);
   NUFHT_LAUNCH_CHECK();
   return 0;
+}
+
+// The local-expansion kernels over `nbox` boxes (g += their contribution): projection per
+// source chunk, reduction of the partial projections per box, evaluation at the targets.
+int launch_loc(const double* rs, const double* ws, const double* cs, int ld_cs, double* gs, int ld_gs, int B,
+               const LocBoxD* d_box, int nbox, const ProjItem* d_proj, int nproj, const EvalItem* d_eval, int neval,
+               double* d_partial, double* d_cheb, int K, int nu_int, double sgn, cudaStream_t st) {
+  const int KL1 = K + 1;
+  const int maxo = nu_int / 2 + K + (nu_int & 1);
+  if (KL1 > kLocThreads * kLocMaxNL || maxo > 2304) return NUFHT_E_TOO_LARGE;
+  // columns per projection CTA: the widest power of two (<= 32, <= B) for which each thread
+  // owns one order, or, for very large degrees, at most kLocMaxNL orders
+  const int cap = KL1 <= kLocThreads ? kLocThreads : kLocThreads * kLocMaxNL;
+  int BT = 32;
+  while (BT > 1 && KL1 * BT > cap) BT >>= 1;
+  BT = std::max(1, std::min(BT, B));
+  const int LS = kLocThreads / BT;
+  const int NL = (KL1 + LS - 1) / LS;
+  if (NL > kLocMaxNL) return NUFHT_E_TOO_LARGE;
+  const int chunk = (int)std::min<size_t>(kLocChunk, kLocSmemDoubles / (size_t)(KL1 + BT));
+  const size_t sm = sizeof(double) * ((size_t)KL1 * chunk + (size_t)chunk * BT);
+  dim3 g((unsigned)nproj, (unsigned)((B + BT - 1) / BT));
+  {
+    PhaseScope ps(kPhaseLocProj, st);
+    if (NL == 1) {
+      if (sm > 48 * 1024) cudaFuncSetAttribute(k_loc_proj<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k_loc_proj<1><<<g, kLocThreads, sm, st>>>(rs, cs, ld_cs, B, d_box, d_proj, KL1, nu_int & 1, d_partial, BT,
+                                               chunk);
+    } else {
+      if (sm > 48 * 1024)
+        cudaFuncSetAttribute(k_loc_proj<kLocMaxNL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k_loc_proj<kLocMaxNL><<<g, kLocThreads, sm, st>>>(rs, cs, ld_cs, B, d_box, d_proj, KL1, nu_int & 1,
+                                                        d_partial, BT, chunk);
+    }
+    NUFHT_LAUNCH_CHECK();
+    long long tot = (long long)nbox * KL1 * B;
+    k_loc_reduce<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_box, nbox, KL1, B, d_partial, d_cheb);
+    NUFHT_LAUNCH_CHECK();
+  }
+  PhaseScope ps(kPhaseLocEval, st);
+  if (maxo <= 64) return launch_loc_eval_t<64>(ws, gs, ld_gs, B, d_box, d_eval, neval, d_cheb, K, nu_int, sgn, st);
+  if (maxo <= 160) return launch_loc_eval_t<160>(ws, gs, ld_gs, B, d_box, d_eval, neval, d_cheb, K, nu_int, sgn, st);
+  if (maxo <= 640) return launch_loc_eval_t<640>(ws, gs, ld_gs, B, d_box, d_eval, neval, d_cheb, K, nu_int, sgn, st);
+  if (maxo <= 1280)
+    return launch_loc_eval_t<1280>(ws, gs, ld_gs, B, d_box, d_eval, neval, d_cheb, K, nu_int, sgn, st);
+  return launch_loc_eval_t<2304>(ws, gs, ld_gs, B, d_box, d_eval, neval, d_cheb, K, nu_int, sgn, st);
 }
 
 }  // namespace
@@ -564,28 +615,8 @@ int DevicePlan::run(const double* cs, int ld_cs, double* gs, int ld_gs, int B, c
   const double sgn = sign;
   // ---- local boxes
   if (!locb.empty()) {
-    if (KL1 > 256) return NUFHT_E_TOO_LARGE;
-    int BT = 32;
-    while (BT > 1 && KL1 * BT > 256) BT >>= 1;
-    BT = std::min(BT, B);
-    dim3 g((unsigned)proj.size(), (unsigned)((B + BT - 1) / BT));
-    size_t sm = sizeof(double) * (KL1 * kLocChunk + kLocChunk * BT);
-    {
-      PhaseScope ps(kPhaseLocProj, st);
-      if (sm > 48 * 1024) cudaFuncSetAttribute(k_loc_proj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      k_loc_proj<<<g, 256, sm, st>>>(d_rs, cs, ld_cs, B, d_locb, d_proj, KL1, (nu2 / 2) & 1, d_partial, BT);
-      NUFHT_LAUNCH_CHECK();
-      long long tot = (long long)locb.size() * KL1 * B;
-      k_loc_reduce<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_locb, (int)locb.size(), KL1, B, d_partial,
-                                                                   d_cheb);
-      NUFHT_LAUNCH_CHECK();
-    }
-    int maxo = (nu2 / 2) / 2 + P.K_loc + ((nu2 / 2) & 1);
-    PhaseScope ps(kPhaseLocEval, st);
-    if (maxo <= 64) rc = launch_loc_eval<64>(*this, gs, ld_gs, B, st, sgn);
-    else if (maxo <= 160) rc = launch_loc_eval<160>(*this, gs, ld_gs, B, st, sgn);
-    else if (maxo <= 512) rc = launch_loc_eval<512>(*this, gs, ld_gs, B, st, sgn);
-    else return NUFHT_E_TOO_LARGE;
+    rc = launch_loc(d_rs, d_ws, cs, ld_cs, gs, ld_gs, B, d_locb, (int)locb.size(), d_proj, (int)proj.size(), d_eval,
+                    (int)eval.size(), d_partial, d_cheb, P.K_loc, nu2 / 2, sgn, st);
     if (rc) return rc;
   }
   // ---- asymptotic boxes
@@ -612,31 +643,8 @@ int DevicePlan::run(const double* cs, int ld_cs, double* gs, int ld_gs, int B, c
 int run_loc_box(const double* rs, const double* ws, const double* cs, int ld_cs, double* gs, int ld_gs,
                 int B, const LocBoxD* d_box, const ProjItem* d_proj, int nproj, const EvalItem* d_eval,
                 int neval, double* d_partial, double* d_cheb, int K, int nu_int, cudaStream_t st) {
-  const int KL1 = K + 1;
-  if (KL1 > 256) return NUFHT_E_TOO_LARGE;
-  int BT = 32;
-  while (BT > 1 && KL1 * BT > 256) BT >>= 1;
-  BT = std::min(BT, B);
-  size_t sm = sizeof(double) * (KL1 * kLocChunk + kLocChunk * BT);
-  if (sm > 48 * 1024) cudaFuncSetAttribute(k_loc_proj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_loc_proj<<<dim3((unsigned)nproj, (unsigned)((B + BT - 1) / BT)), 256, sm, st>>>(
-      rs, cs, ld_cs, B, d_box, d_proj, KL1, nu_int & 1, d_partial, BT);
-  NUFHT_LAUNCH_CHECK();
-  long long tot = (long long)KL1 * B;
-  k_loc_reduce<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_box, 1, KL1, B, d_partial, d_cheb);
-  NUFHT_LAUNCH_CHECK();
-  const int maxo = nu_int / 2 + K + (nu_int & 1);
-  size_t sme = sizeof(double) * KL1 * B;
-  auto eval = [&](auto kern) -> int {
-    if (sme > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sme);
-    kern<<<(unsigned)neval, kLocTargets, sme, st>>>(ws, gs, ld_gs, B, d_box, d_eval, d_cheb, K, nu_int, 1.0);
-    NUFHT_LAUNCH_CHECK();
-    return 0;
-  };
-  if (maxo <= 64) return eval(k_loc_eval<64>);
-  if (maxo <= 160) return eval(k_loc_eval<160>);
-  if (maxo <= 512) return eval(k_loc_eval<512>);
-  return NUFHT_E_TOO_LARGE;
+  return launch_loc(rs, ws, cs, ld_cs, gs, ld_gs, B, d_box, 1, d_proj, nproj, d_eval, neval, d_partial, d_cheb, K,
+                    nu_int, 1.0, st);
 }
 
 int run_besselj(double nu, const double* x, double* out, long count, cudaStream_t st) {

@@ -11,31 +11,39 @@
 namespace hankel {
 
 constexpr int kLocSources = 2048;  // sources per projection work item
-constexpr int kLocChunk = 64;      // sources staged per round
+constexpr int kLocChunk = 64;      // sources staged per round, at most
 constexpr int kLocTargets = 128;   // targets per evaluation CTA
+constexpr int kLocThreads = 256;   // threads of a projection CTA
+constexpr int kLocMaxNL = 16;      // expansion orders per projection thread, at most
 
 // Partial projections over one source chunk; Chebyshev polynomials by the three-term
-// recurrence T_{n+1} = 2 x T_n - T_{n-1}.
-__global__ void __launch_bounds__(256) k_loc_proj(
+// recurrence T_{n+1} = 2 x T_n - T_{n-1}.  Thread (l_out, t_out) owns column t0 + t_out and
+// the orders l_out + q LS, q < NL (LS = kLocThreads / BT): NL = 1 for the usual degrees,
+// up to kLocMaxNL for the Wimp degrees of very large orders (hundreds).  `chunk` sources are
+// staged per round so that the KL1 x chunk table fits in shared memory.
+template <int NL>
+__global__ void __launch_bounds__(kLocThreads) k_loc_proj(
     const double* __restrict__ rs, const double* __restrict__ cs, int ld_cs, int B,
     const LocBoxD* __restrict__ boxes, const ProjItem* __restrict__ items, int KL1, int odd,
-    double* __restrict__ partial, int BT) {
+    double* __restrict__ partial, int BT, int chunk) {
   const ProjItem it = items[blockIdx.x];
   const LocBoxD bx = boxes[it.box];
   const int t0 = blockIdx.y * BT;
   const int tid = threadIdx.x;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* sT = reinterpret_cast<double*>(smem_raw);  // [KL1][kLocChunk]
-  double* sC = sT + KL1 * kLocChunk;                  // [kLocChunk][BT]
+  double* sT = reinterpret_cast<double*>(smem_raw);  // [KL1][chunk]
+  double* sC = sT + (size_t)KL1 * chunk;              // [chunk][BT]
+  const int LS = kLocThreads / BT;
   const int l_out = tid / BT, t_out = tid - l_out * BT;
-  const bool has_out = l_out < KL1;
-  double acc = 0.0;
+  double acc[NL];
+#pragma unroll
+  for (int q = 0; q < NL; ++q) acc[q] = 0.0;
   // A box whose sources all sit at r = 0 has r_end = 0; then only the l = 0 term survives
   // (J_l(0) = 0 for l >= 1) and any x works.  The reference divides by zero there.
   const double inv_end = bx.r_end > 0.0 ? 1.0 / bx.r_end : 0.0;
-  for (int s0 = 0; s0 < it.nj; s0 += kLocChunk) {
-    const int ns = min(kLocChunk, it.nj - s0);
-    for (int s = tid; s < kLocChunk; s += blockDim.x) {
+  for (int s0 = 0; s0 < it.nj; s0 += chunk) {
+    const int ns = min(chunk, it.nj - s0);
+    for (int s = tid; s < chunk; s += blockDim.x) {
       if (s < ns) {
         double x = rs[it.j0 + s0 + s] * inv_end;
         x = fmin(fmax(x, -1.0), 1.0);
@@ -55,29 +63,39 @@ __global__ void __launch_bounds__(256) k_loc_proj(
           }
           int order = odd ? 2 * l + 1 : 2 * l;
           if (nn == order) {
-            sT[l * kLocChunk + s] = odd ? 2.0 * Tn : (l == 0 ? Tn : 2.0 * Tn);
+            sT[(size_t)l * chunk + s] = odd ? 2.0 * Tn : (l == 0 ? Tn : 2.0 * Tn);
             ++l;
           }
         }
       } else {
-        for (int l = 0; l < KL1; ++l) sT[l * kLocChunk + s] = 0.0;
+        for (int l = 0; l < KL1; ++l) sT[(size_t)l * chunk + s] = 0.0;
       }
     }
-    for (int e = tid; e < kLocChunk * BT; e += blockDim.x) {
-      int tt = e / kLocChunk, s = e - tt * kLocChunk;
-      sC[s * BT + tt] =
-          (s < ns && t0 + tt < B) ? cs[(size_t)(t0 + tt) * ld_cs + it.j0 + s0 + s] : 0.0;
+    for (int e = tid; e < chunk * BT; e += blockDim.x) {
+      int tt = e / chunk, s = e - tt * chunk;
+      sC[s * BT + tt] = (s < ns && t0 + tt < B) ? cs[(size_t)(t0 + tt) * ld_cs + it.j0 + s0 + s] : 0.0;
     }
     __syncthreads();
-    if (has_out) {
-      const double* Tl = sT + l_out * kLocChunk;
+#pragma unroll
+    for (int q = 0; q < NL; ++q) {
+      const int l = l_out + q * LS;
+      if (l < KL1) {
+        const double* Tl = sT + (size_t)l * chunk;
+        double a = acc[q];
 #pragma unroll 8
-      for (int s = 0; s < kLocChunk; ++s) acc = fma(Tl[s], sC[s * BT + t_out], acc);
+        for (int s = 0; s < ns; ++s) a = fma(Tl[s], sC[s * BT + t_out], a);
+        acc[q] = a;
+      }
     }
     __syncthreads();
   }
-  if (has_out && t0 + t_out < B)
-    partial[((size_t)blockIdx.x * KL1 + l_out) * B + t0 + t_out] = acc;
+  if (t0 + t_out < B) {
+#pragma unroll
+    for (int q = 0; q < NL; ++q) {
+      const int l = l_out + q * LS;
+      if (l < KL1) partial[((size_t)blockIdx.x * KL1 + l) * B + t0 + t_out] = acc[q];
+    }
+  }
 }
 
 __global__ void k_loc_reduce(const LocBoxD* __restrict__ boxes, int nbox, int KL1, int B,
@@ -93,43 +111,54 @@ __global__ void k_loc_reduce(const LocBoxD* __restrict__ boxes, int nbox, int KL
   cheb[e] = s;
 }
 
+// Evaluation at the box's targets: J_0 .. J_maxo at z = k r_end / 2 by Miller's algorithm
+// (local array of MAXO + 1 values per thread), then g[i,t] += sum_l b_l C[l,t] with
+// b_l = J_{l0+odd+l} J_{|l-l0|} (-1)^{max(l-l0,0)}.  The coefficients C of the box are
+// staged in shared memory for BTC columns at a time.
 template <int MAXO>
 __global__ void __launch_bounds__(kLocTargets) k_loc_eval(
     const double* __restrict__ ws, double* __restrict__ gs, int ld_gs, int B,
     const LocBoxD* __restrict__ boxes, const EvalItem* __restrict__ items,
-    const double* __restrict__ cheb, int K, int nu_int, double sgn) {
+    const double* __restrict__ cheb, int K, int nu_int, double sgn, int BTC) {
   const EvalItem it = items[blockIdx.x];
   const LocBoxD bx = boxes[it.box];
   const int KL1 = K + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* s_cheb = reinterpret_cast<double*>(smem_raw);  // [KL1][B]
-  for (int e = threadIdx.x; e < KL1 * B; e += blockDim.x)
-    s_cheb[e] = cheb[(size_t)it.box * KL1 * B + e];
-  __syncthreads();
+  double* s_cheb = reinterpret_cast<double*>(smem_raw);  // [KL1][BTC]
   const int tid = threadIdx.x;
-  if (tid >= it.ni) return;
-  const int i = it.i0 + tid;
+  const bool has = tid < it.ni;
+  const int i = it.i0 + (has ? tid : 0);
   const int l0 = nu_int / 2, odd = nu_int & 1;
   const int maxo = l0 + K + odd;
   double J[MAXO + 1];
-  double z = ws[i] * bx.r_end / 2.0;
-  if (z < 1e-30) {
-    for (int q = 0; q <= maxo; ++q) J[q] = 0.0;
-    J[0] = 1.0;
-  } else {
-    bessel_j_orders(maxo, z, J);
+  if (has) {
+    double z = ws[i] * bx.r_end / 2.0;
+    if (z < 1e-30) {
+      for (int q = 0; q <= maxo; ++q) J[q] = 0.0;
+      J[0] = 1.0;
+    } else {
+      bessel_j_orders(maxo, z, J);
+    }
   }
-  double bl[MAXO + 1];
-  for (int l = 0; l <= K; ++l) {
-    int lo = l > l0 ? l - l0 : l0 - l;
-    double v = J[l0 + odd + l] * J[lo];
-    if (l > l0 && ((l - l0) & 1)) v = -v;
-    bl[l] = v;
-  }
-  for (int t = 0; t < B; ++t) {
-    double acc = 0.0;
-    for (int l = 0; l <= K; ++l) acc = fma(bl[l], s_cheb[l * B + t], acc);
-    atomicAdd(&gs[(size_t)t * ld_gs + i], sgn * acc);
+  for (int tb = 0; tb < B; tb += BTC) {
+    const int nt = min(BTC, B - tb);
+    __syncthreads();
+    for (int e = tid; e < KL1 * nt; e += blockDim.x) {
+      int l = e / nt, tt = e - l * nt;
+      s_cheb[l * BTC + tt] = cheb[((size_t)it.box * KL1 + l) * B + tb + tt];
+    }
+    __syncthreads();
+    if (!has) continue;
+    for (int tt = 0; tt < nt; ++tt) {
+      double acc = 0.0;
+      for (int l = 0; l <= K; ++l) {
+        int lo = l > l0 ? l - l0 : l0 - l;
+        double v = J[l0 + odd + l] * J[lo];
+        if (l > l0 && ((l - l0) & 1)) v = -v;
+        acc = fma(v, s_cheb[l * BTC + tt], acc);
+      }
+      atomicAdd(&gs[(size_t)(tb + tt) * ld_gs + i], sgn * acc);
+    }
   }
 }
 
