@@ -208,52 +208,106 @@ void drop_device_state(const NufhtPlan* plan) {
 }
 
 // Run D on cs/gs that may be host or device pointers (synchronous, legacy stream).
+// Device buffer of at least `need` bytes (grown, never shrunk).
+int stage_buffer(double** buf, size_t* have, size_t need) {
+  if (need <= *have) return 0;
+  cudaFree(*buf);
+  *buf = nullptr;
+  *have = 0;
+  if (cudaMalloc((void**)buf, need) != cudaSuccess) return NUFHT_E_CUDA;
+  *have = need;
+  return 0;
+}
+
+// Column blocks of the pipelined host-buffer path: the transfers of one block overlap the
+// transform of another, so large calls are cut into 2 to 4 equal blocks (equal, so that
+// the FFT plans made for one width serve every block) of at least 16 columns (narrower
+// blocks spread and interpolate less efficiently).
+int pipeline_blocks(const DevicePlan* D, int B) {
+  static const int forced = [] {  // NUFHT_B200_PIPELINE_BLOCKS=1 turns the pipeline off (tuning)
+    const char* e = std::getenv("NUFHT_B200_PIPELINE_BLOCKS");
+    return e ? std::atoi(e) : 0;
+  }();
+  if (forced > 0) return (B % forced == 0) ? forced : 1;
+  const double bytes = 8.0 * ((double)D->m + (double)D->n) * (double)B;
+  if (bytes < 64.0 * 1024 * 1024) return 1;
+  for (int nb : {4, 3, 2})
+    if (B % nb == 0 && B / nb >= 16) return nb;
+  return 1;
+}
+
 int run_any(DevicePlan* D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, bool zero) {
   std::lock_guard<std::mutex> lk(D->mu);
   if (cudaSetDevice(D->device) != cudaSuccess) return NUFHT_E_CUDA;
   cudaStream_t st = 0;
   const bool cdev = is_device_ptr(cs), gdev = is_device_ptr(gs);
-  const double* dc = cs;
-  double* dg = gs;
-  int ldc = ld_cs, ldg = ld_gs;
-  if (!cdev) {
-    size_t need = sizeof(double) * (size_t)D->m * (size_t)B;
-    if (need > D->stage_c_bytes) {
-      cudaFree(D->d_stage_c);
-      D->d_stage_c = nullptr;
-      D->stage_c_bytes = 0;
-      if (cudaMalloc((void**)&D->d_stage_c, need) != cudaSuccess) return NUFHT_E_CUDA;
-      D->stage_c_bytes = need;
-    }
-    if (cudaMemcpy2DAsync(D->d_stage_c, sizeof(double) * D->m, cs, sizeof(double) * (size_t)ld_cs,
-                          sizeof(double) * D->m, B, cudaMemcpyHostToDevice, st) != cudaSuccess)
-      return NUFHT_E_CUDA;
-    dc = D->d_stage_c;
-    ldc = D->m;
+  int rc;
+  if (cdev && gdev) {
+    rc = D->run(cs, ld_cs, gs, ld_gs, B, st, zero);
+    if (rc) return rc;
+    return cudaStreamSynchronize(st) == cudaSuccess ? 0 : NUFHT_E_CUDA;
   }
-  if (!gdev) {
-    size_t need = sizeof(double) * (size_t)D->n * (size_t)B;
-    if (need > D->stage_g_bytes) {
-      cudaFree(D->d_stage_g);
-      D->d_stage_g = nullptr;
-      D->stage_g_bytes = 0;
-      if (cudaMalloc((void**)&D->d_stage_g, need) != cudaSuccess) return NUFHT_E_CUDA;
-      D->stage_g_bytes = need;
-    }
-    dg = D->d_stage_g;
-    ldg = D->n;
-    if (!zero &&
-        cudaMemcpy2DAsync(dg, sizeof(double) * D->n, gs, sizeof(double) * (size_t)ld_gs,
-                          sizeof(double) * D->n, B, cudaMemcpyHostToDevice, st) != cudaSuccess)
+  if ((rc = stage_buffer(&D->d_stage_c, &D->stage_c_bytes, cdev ? 0 : sizeof(double) * (size_t)D->m * B)) ||
+      (rc = stage_buffer(&D->d_stage_g, &D->stage_g_bytes, gdev ? 0 : sizeof(double) * (size_t)D->n * B)))
+    return rc;
+  const double* dc = cdev ? cs : D->d_stage_c;
+  double* dg = gdev ? gs : D->d_stage_g;
+  const int ldc = cdev ? ld_cs : D->m, ldg = gdev ? ld_gs : D->n;
+  const int nb = zero ? pipeline_blocks(D, B) : 1;
+  if (nb == 1) {
+    if (!cdev && cudaMemcpy2DAsync(D->d_stage_c, sizeof(double) * D->m, cs, sizeof(double) * (size_t)ld_cs,
+                                   sizeof(double) * D->m, B, cudaMemcpyHostToDevice, st) != cudaSuccess)
       return NUFHT_E_CUDA;
+    if (!gdev && !zero &&
+        cudaMemcpy2DAsync(dg, sizeof(double) * D->n, gs, sizeof(double) * (size_t)ld_gs, sizeof(double) * D->n, B,
+                          cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return NUFHT_E_CUDA;
+    if ((rc = D->run(dc, ldc, dg, ldg, B, st, zero))) return rc;
+    if (!gdev && cudaMemcpy2DAsync(gs, sizeof(double) * (size_t)ld_gs, dg, sizeof(double) * D->n,
+                                   sizeof(double) * D->n, B, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      return NUFHT_E_CUDA;
+    return cudaStreamSynchronize(st) == cudaSuccess ? 0 : NUFHT_E_CUDA;
   }
-  int rc = D->run(dc, ldc, dg, ldg, B, st, zero);
-  if (rc) return rc;
-  if (!gdev &&
-      cudaMemcpy2DAsync(gs, sizeof(double) * (size_t)ld_gs, dg, sizeof(double) * D->n,
-                        sizeof(double) * D->n, B, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+  // Pipelined: block q's host-to-device copy (copy_in), transform (st) and device-to-host
+  // copy (copy_out) overlap the neighbouring blocks' stages.
+  if (!D->copy_in) {
+    if (cudaStreamCreateWithFlags(&D->copy_in, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&D->copy_out, cudaStreamNonBlocking) != cudaSuccess)
+      return NUFHT_E_CUDA;
+    for (int q = 0; q < 4; ++q)
+      if (cudaEventCreateWithFlags(&D->ev_in[q], cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventCreateWithFlags(&D->ev_done[q], cudaEventDisableTiming) != cudaSuccess)
+        return NUFHT_E_CUDA;
+  }
+  const int Bc = B / nb;
+  // the copy streams start after all earlier work on st (e.g. a previous call's transform)
+  if (cudaEventRecord(D->ev_done[0], st) != cudaSuccess || cudaStreamWaitEvent(D->copy_in, D->ev_done[0], 0) ||
+      cudaStreamWaitEvent(D->copy_out, D->ev_done[0], 0))
     return NUFHT_E_CUDA;
-  if (cudaStreamSynchronize(st) != cudaSuccess) return NUFHT_E_CUDA;
+  for (int q = 0; q < nb; ++q) {
+    if (!cdev) {
+      if (cudaMemcpy2DAsync(D->d_stage_c + (size_t)q * Bc * D->m, sizeof(double) * D->m,
+                            cs + (size_t)q * Bc * ld_cs, sizeof(double) * (size_t)ld_cs, sizeof(double) * D->m, Bc,
+                            cudaMemcpyHostToDevice, D->copy_in) != cudaSuccess)
+        return NUFHT_E_CUDA;
+    }
+    if (cudaEventRecord(D->ev_in[q], D->copy_in) != cudaSuccess) return NUFHT_E_CUDA;
+  }
+  for (int q = 0; q < nb; ++q) {
+    if (cudaStreamWaitEvent(st, D->ev_in[q], 0) != cudaSuccess) return NUFHT_E_CUDA;
+    if ((rc = D->run(dc + (size_t)q * Bc * ldc, ldc, dg + (size_t)q * Bc * ldg, ldg, Bc, st, true))) return rc;
+    if (cudaEventRecord(D->ev_done[q], st) != cudaSuccess) return NUFHT_E_CUDA;
+    if (!gdev) {
+      if (cudaStreamWaitEvent(D->copy_out, D->ev_done[q], 0) != cudaSuccess ||
+          cudaMemcpy2DAsync(gs + (size_t)q * Bc * ld_gs, sizeof(double) * (size_t)ld_gs,
+                            D->d_stage_g + (size_t)q * Bc * D->n, sizeof(double) * D->n, sizeof(double) * D->n, Bc,
+                            cudaMemcpyDeviceToHost, D->copy_out) != cudaSuccess)
+        return NUFHT_E_CUDA;
+    }
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess || cudaStreamSynchronize(D->copy_out) != cudaSuccess ||
+      cudaStreamSynchronize(D->copy_in) != cudaSuccess)
+    return NUFHT_E_CUDA;
   return 0;
 }
 

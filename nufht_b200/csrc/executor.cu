@@ -17,6 +17,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <utility>
@@ -223,8 +224,21 @@ void DevicePlan::build_lists() {
   int Wc[3];
   for (int c = 0; c < 3; ++c) Wc[c] = spread_width(P.tol, kSigmas[c]);
   // In FP32 the deconvolution by psi-hat amplifies rounding by psi-hat(0)/psi-hat(pi/sigma):
-  // about 3 at sigma = 2, 26 at 1.5 and 1100 at 1.25, so mixed precision keeps sigma = 2.
-  if (mixed_asy) Wc[1] = Wc[2] = 0;
+  // about 3 at sigma = 2, 26 at 1.5 and 1100 at 1.25, so mixed precision keeps sigma = 2
+  // unless NUFHT_B200_MIXED_SIGMAS lists the classes to allow (tuning: "2,1.5").
+  if (mixed_asy) {
+    static const int allowed = [] {
+      const char* e = std::getenv("NUFHT_B200_MIXED_SIGMAS");
+      int mask = 1;
+      if (e) {
+        if (std::strstr(e, "1.5")) mask |= 2;
+        if (std::strstr(e, "1.25")) mask |= 4;
+      }
+      return mask;
+    }();
+    if (!(allowed & 2)) Wc[1] = 0;
+    if (!(allowed & 4)) Wc[2] = 0;
+  }
   std::vector<AsyBoxD> tmp;
   for (const HBox& hb : asy_boxes) {
     AsyBoxD d;
@@ -269,7 +283,7 @@ void DevicePlan::build_lists() {
     d.h = M_PI / (sigma * S);
     long long half = (long long)std::ceil(X / d.h + 0.5 * Wb);
     d.half = (int)half;
-    d.n2 = (int)fft_len(std::max<long long>((long long)std::ceil(sigma * (2 * half + 1)), 2 * kSpreadTile));
+    d.n2 = (int)fft_len(std::max<long long>((long long)std::ceil(sigma * (2 * half + 1)), (long long)kMinFft));
     // Dense boxes (many sources per grid cell) are spread by source chunks.
     auto l0_of = [&](int j) { return (long long)std::ceil((rs[j] - d.C) / d.h - 0.5 * Wb); };
     auto first_ge = [&](long long lo) {
@@ -455,6 +469,12 @@ DevicePlan::~DevicePlan() {
   cudaFree(d_corr); cudaFree(d_post);
   cudaFree(d_grid); cudaFree(d_partial); cudaFree(d_cheb); cudaFree(d_fft_work);
   cudaFree(d_stage_c); cudaFree(d_stage_g);
+  if (copy_in) cudaStreamDestroy(copy_in);
+  if (copy_out) cudaStreamDestroy(copy_out);
+  for (int q = 0; q < 4; ++q) {
+    if (ev_in[q]) cudaEventDestroy(ev_in[q]);
+    if (ev_done[q]) cudaEventDestroy(ev_done[q]);
+  }
   if (prev >= 0) cudaSetDevice(prev);
 }
 

@@ -137,6 +137,9 @@ struct DevicePlan {
   double* d_stage_c = nullptr;
   double* d_stage_g = nullptr;
   size_t stage_c_bytes = 0, stage_g_bytes = 0;
+  // copy streams and events of the pipelined host-buffer path (created on first use)
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t ev_in[4] = {}, ev_done[4] = {};
 
   std::mutex mu;
 

@@ -28,6 +28,7 @@
 namespace hankel {
 
 constexpr int kSpreadTile = 16;     // cells owned by one mode-0 spreading CTA
+constexpr int kMinFft = 32;         // smallest FFT length of a box
 constexpr int kSpreadChunk = 64;    // sources staged in shared memory per round
 constexpr int kChunkSources = 2048; // sources per mode-1 work item, at most
 constexpr int kTileMaxSources = 4096;
