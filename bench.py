@@ -392,6 +392,14 @@ def main():
         roofline["fp64"] = {"achieved": ach_tf, "peak": fp64_peak.value, "unit": "TFLOP/s",
                             "frac": ach_tf / fp64_peak.value if fp64_peak.value > 0 else None,
                             "peak_source": "measured FP64 FMA probe (nufht_b200_fp64_peak)"}
+    elif dom in flops:
+        # single-precision spreading / interpolation: issue-bound on packed FP32 FMAs
+        fp32_peak = ctypes.c_double(0.0)
+        lib.nufht_b200_fp32_peak(ctypes.byref(fp32_peak))
+        ach_tf = flops[dom] / t_dom / 1e12
+        roofline["fp32"] = {"achieved": ach_tf, "peak": fp32_peak.value, "unit": "TFLOP/s",
+                            "frac": ach_tf / fp32_peak.value if fp32_peak.value > 0 else None,
+                            "peak_source": "measured FP32 packed-FMA probe (nufht_b200_fp32_peak)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -230,6 +230,9 @@ int nufht_b200_plan_stats(const NufhtDevicePlan *plan, double *out, int n);
 
 /* Measured FP64 fused-multiply-add throughput of the current device (TFLOP/s). */
 int nufht_b200_fp64_peak(double *tflops);
+/* Measured FP32 throughput of the packed two-lane multiply-add (fma.rn.f32x2) that the
+ * single-precision asymptotic kernels use (TFLOP/s). */
+int nufht_b200_fp32_peak(double *tflops);
 
 /* No counterpart in the reference.  Allocation-free variant of add_loc_batch for callers
  * that cannot call cudaMalloc at call time (a fixed memory budget or pool, allocation

@@ -118,6 +118,7 @@ def _declare(lib):
         "nufht_b200_set_phase_timing": (None, [ctypes.c_int]),
         "nufht_b200_plan_stats": (ctypes.c_int, [vp, c_double_p, ctypes.c_int]),
         "nufht_b200_fp64_peak": (ctypes.c_int, [c_double_p]),
+        "nufht_b200_fp32_peak": (ctypes.c_int, [c_double_p]),
         "nufht_b200_add_loc_batch_noalloc": (ctypes.c_int, [vp, ctypes.c_double, vp, vp, vp, ctypes.c_int,
                                                             ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                             ctypes.c_int, vp]),

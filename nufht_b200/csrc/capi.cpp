@@ -685,3 +685,8 @@ extern "C" int nufht_b200_fp64_peak(double* tflops) {
   if (!tflops) return -400;
   return hankel::fp64_peak(tflops);
 }
+
+extern "C" int nufht_b200_fp32_peak(double* tflops) {
+  if (!tflops) return -400;
+  return hankel::fp32_peak(tflops);
+}

@@ -196,6 +196,8 @@ namespace hankel {
 // Algorithmic work of a plan per batch column, for roofline accounting (see stats order in
 // nufht_b200_plan_stats).
 void plan_stats(const DevicePlan& D, double* out, int n);
+// Measured FP32 (packed f32x2) fused-multiply-add throughput of the current device in TFLOP/s.
+int fp32_peak(double* tflops);
 // Measured FP64 fused-multiply-add throughput of the current device in TFLOP/s.
 int fp64_peak(double* tflops);
 }  // namespace hankel

@@ -53,7 +53,66 @@ __global__ void k_fp64_fma(double* out, int iters, double a, double b) {
   double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
   if (s == 12345.678) out[0] = s;  // keeps the loop alive
 }
+// Packed two-lane FP32 multiply-add (fma.rn.f32x2), the instruction the single-precision
+// asymptotic kernels issue.
+__device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b,
+                                                    unsigned long long c) {
+  unsigned long long d;
+  asm volatile("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__global__ void k_fp32_fma(float* out, int iters, float a, float b) {
+  const unsigned long long pa = (unsigned long long)__float_as_uint(a) | ((unsigned long long)__float_as_uint(a) << 32);
+  const unsigned long long pb = (unsigned long long)__float_as_uint(b) | ((unsigned long long)__float_as_uint(b) << 32);
+  unsigned long long x[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+    x[q] = (unsigned long long)__float_as_uint((float)(threadIdx.x + q)) |
+           ((unsigned long long)__float_as_uint((float)(threadIdx.x + 2 * q)) << 32);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) x[q] = ffma2(x[q], pa, pb);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) s += __uint_as_float((unsigned)(x[q] & 0xffffffffull)) + __uint_as_float((unsigned)(x[q] >> 32));
+  if (s == 12345.678f) out[0] = s;  // keeps the loop alive
+}
+
+template <class Launch>
+int time_probe(Launch launch, float* ms_out) {
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  launch(64);  // warm up
+  cudaEventRecord(e0);
+  launch(4096);
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms_out = ms;
+  return (cudaGetLastError() != cudaSuccess || ms <= 0.f) ? NUFHT_E_CUDA : 0;
+}
 }  // namespace
+
+int fp32_peak(double* tflops) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  float* d = nullptr;
+  if (cudaMalloc(&d, sizeof(float)) != cudaSuccess) return NUFHT_E_CUDA;
+  const int blocks = sms * 8, threads = 256;
+  float ms = 0.f;
+  int rc = time_probe([&](int it) { k_fp32_fma<<<blocks, threads>>>(d, it, 0.999999f, 1e-9f); }, &ms);
+  cudaFree(d);
+  if (rc) return rc;
+  // 8 chains x 2 lanes x 2 flops per packed FMA
+  *tflops = 2.0 * 2.0 * 8.0 * 4096.0 * blocks * threads / (ms * 1e-3) / 1e12;
+  return 0;
+}
 
 int fp64_peak(double* tflops) {
   int dev = 0, sms = 0;
