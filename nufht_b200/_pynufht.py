@@ -6,10 +6,13 @@ Same three functions, argument meaning, result layout and exceptions:
   nufht_batch(nu, rs, cs, ws, tol=1e-8)      -> ndarray (n, batch), C order
   nufht_batch_loop(nu, rs, cs, ws, tol=1e-8) -> ndarray (n, batch), one transform per column
 
-Each call plans (on the host) and runs the transform on the GPU through the C ABI of
-libnufht_b200.so, as the reference plans and runs on the CPU per call (src/_pynufht.c:186).
+Each call runs the transform on the GPU through the C ABI of libnufht_b200.so.  The
+reference plans on the CPU per call (src/_pynufht.c:186); `nufht_batch` here keeps the last
+few plans (keyed by order, tolerance and the grids' contents) and reuses them.
 """
 import ctypes
+import hashlib
+import os
 
 import numpy as np
 
@@ -49,6 +52,61 @@ def _check_batch(rs, cs):
     return cs
 
 
+class _PlanCache:
+    """The last few plans, keyed by (nu, tol, grids).  The reference plans on every call
+    (src/_pynufht.c:186); repeated calls on the same grids here reuse the host plan and its
+    device state (work lists, FFT plans, workspace).  The grids are kept alive with the plan,
+    which borrows them."""
+
+    def __init__(self, size=4):
+        self.size = size
+        self.entries = []  # (key, plan, rs, ws), most recent last
+
+    @staticmethod
+    def key(nu, tol, rs, ws):
+        h = hashlib.blake2b(digest_size=16)
+        h.update(rs.tobytes())
+        h.update(ws.tobytes())
+        # the precision switch of the reference entry points is read when a plan first runs
+        return (float(nu), float(tol), rs.shape[0], ws.shape[0], h.digest(),
+                os.environ.get("NUFHT_B200_PRECISION", ""))
+
+    def get(self, nu, tol, rs, ws):
+        k = self.key(nu, tol, rs, ws)
+        for q, (kk, plan, r, w) in enumerate(self.entries):
+            if kk == k:
+                self.entries.append(self.entries.pop(q))
+                return plan
+        lib = L.lib()
+        opt = L.options(tol=float(tol))
+        plan = L.NufhtPlan()
+        rs = rs.copy()
+        ws = ws.copy()
+        if lib.nufht_plan_init(ctypes.byref(plan), float(nu), L.dptr(rs), rs.shape[0], L.dptr(ws), ws.shape[0],
+                               ctypes.byref(opt)) != 0:
+            lib.nufht_plan_free(ctypes.byref(plan))
+            raise RuntimeError("nufht_plan_init failed")
+        self.entries.append((k, plan, rs, ws))
+        while len(self.entries) > self.size:
+            _, old, _, _ = self.entries.pop(0)
+            lib.nufht_plan_free(ctypes.byref(old))
+        return plan
+
+    def clear(self):
+        lib = L.lib()
+        for _, plan, _, _ in self.entries:
+            lib.nufht_plan_free(ctypes.byref(plan))
+        self.entries = []
+
+
+_plans = _PlanCache()
+
+
+def clear_plan_cache():
+    """Release the cached plans (and their device memory)."""
+    _plans.clear()
+
+
 def nufht_batch(nu, rs, cs, ws, tol=1e-8):
     """Batched transform through nufht_plan_init / nufht_batch (src/_pynufht.c:144-239)."""
     lib = L.lib()
@@ -57,18 +115,11 @@ def nufht_batch(nu, rs, cs, ws, tol=1e-8):
     cs = _check_batch(rs, cs)
     cs = np.asfortranarray(cs)  # column-major, as the reference forces (src/_pynufht.c:156)
     m, n, batch = rs.shape[0], ws.shape[0], cs.shape[1]
-    opt = L.options(tol=float(tol))
-    plan = L.NufhtPlan()
-    if lib.nufht_plan_init(ctypes.byref(plan), float(nu), L.dptr(rs), m, L.dptr(ws), n, ctypes.byref(opt)) != 0:
-        lib.nufht_plan_free(ctypes.byref(plan))
-        raise RuntimeError("nufht_plan_init failed")
-    try:
-        gs = np.empty((n, batch), dtype=np.float64, order="F")
-        ret = lib.nufht_batch(ctypes.byref(plan), L.dptr(cs), m, L.dptr(gs), n, batch, None)
-        if ret != 0:
-            raise RuntimeError("nufht_batch returned %d" % ret)
-    finally:
-        lib.nufht_plan_free(ctypes.byref(plan))
+    plan = _plans.get(nu, tol, rs, ws)
+    gs = np.empty((n, batch), dtype=np.float64, order="F")
+    ret = lib.nufht_batch(ctypes.byref(plan), L.dptr(cs), m, L.dptr(gs), n, batch, None)
+    if ret != 0:
+        raise RuntimeError("nufht_batch returned %d" % ret)
     return np.ascontiguousarray(gs)  # C-order (n, batch) result (src/_pynufht.c:222-237)
 
 

@@ -108,7 +108,7 @@ __device__ __forceinline__ int run_end(const int* a, int n, int s) {
 
 // Shared-memory layout of k_asy_interp.
 struct InterpSmem {
-  size_t mu, y, wt, q0, end, total;
+  size_t mu, y, wt, q0, end, uu, total;
 };
 template <typename T>
 __host__ __device__ inline InterpSmem interp_smem(int W, int NLP, int threads) {
@@ -118,7 +118,8 @@ __host__ __device__ inline InterpSmem interp_smem(int W, int NLP, int threads) {
   L.wt = align16(L.y + (threads > 0 ? (size_t)kInterpChunk * (threads + 1) * sizeof(double) : 0));
   L.q0 = align16(L.wt + (size_t)kInterpChunk * interp_we<T>(W) * sizeof(T));
   L.end = align16(L.q0 + (size_t)kInterpChunk * 4);
-  L.total = align16(L.end + (size_t)kInterpChunk * 4);
+  L.uu = align16(L.end + (size_t)kInterpChunk * 4);
+  L.total = align16(L.uu + (size_t)kInterpChunk * sizeof(double));
   return L;
 }
 
@@ -446,6 +447,7 @@ __global__ void __launch_bounds__(256) k_asy_interp(
   T* s_wt = reinterpret_cast<T*>(smem_raw + L.wt);          // [KC][WE]
   int* s_q0 = reinterpret_cast<int*>(smem_raw + L.q0);      // [KC]
   int* s_end = reinterpret_cast<int*>(smem_raw + L.end);    // [KC]: end of the equal-q0 run
+  double* s_uu = reinterpret_cast<double*>(smem_raw + L.uu);  // [KC]: target position in cells
 
   const int n2 = bx.n2;
   const C2* row[LPT];
@@ -465,26 +467,30 @@ __global__ void __launch_bounds__(256) k_asy_interp(
   // Stage targets [k0, k0 + nk) (all threads; barriers on both sides).
   auto stage = [&](int k0, int nk) {
     __syncthreads();
+    // per target (one thread each): stencil start, and the NLP factors
+    // mu_q = coef_q (k rref)^{-(q + 1/2)} exp(i (phi + k C)) / psi-hat, rotated by i for odd q,
+    // with one square root and one reciprocal per target
     for (int kk = tid; kk < nk; kk += nthr) {
-      double uu = (ws[k0 + kk] - bx.D) * u_scale;
-      int q0 = (int)ceil(uu - 0.5 * W);
-      s_q0[kk] = q0;
-      for (int q = 0; q < WE; ++q)
-        s_wt[kk * WE + q] = q < W ? es_kernel_t((T)(uu - (double)(q0 + q)), ihw, beta) : (T)0;
-    }
-    for (int e = tid; e < nk * NLP; e += nthr) {
-      int kk = e / NLP, q = e - kk * NLP;
-      double k = ws[k0 + kk];
-      double2 ps = post[bx.post_off + (k0 + kk - bx.i0)];
-      // coef_q (k rref)^{-(q + 1/2)}
-      double kr = k * bx.rref;
-      double pw = 1.0 / sqrt(kr), ik = 1.0 / kr;
-      for (int e2 = 0; e2 < q; ++e2) pw *= ik;
-      double sc = P.coef[q] * pw;
-      double mr = sc * ps.x, mi = sc * ps.y;
-      s_mu[kk * NLP + q] = (q & 1) ? cmake<T>((T)-mi, (T)mr) : cmake<T>((T)mr, (T)mi);
+      const double k = ws[k0 + kk];
+      const double uu = (k - bx.D) * u_scale;
+      s_uu[kk] = uu;
+      s_q0[kk] = (int)ceil(uu - 0.5 * W);
+      const double2 ps = post[bx.post_off + (k0 + kk - bx.i0)];
+      const double kr = k * bx.rref;
+      const double ik = 1.0 / kr;
+      double pw = sqrt(ik);
+      for (int q = 0; q < NLP; ++q, pw *= ik) {
+        const double sc = P.coef[q] * pw;
+        const double mr = sc * ps.x, mi = sc * ps.y;
+        s_mu[kk * NLP + q] = (q & 1) ? cmake<T>((T)-mi, (T)mr) : cmake<T>((T)mr, (T)mi);
+      }
     }
     __syncthreads();
+    // kernel weights over all (target, tap) pairs
+    for (int e = tid; e < nk * WE; e += nthr) {
+      const int kk = e / WE, q = e - kk * WE;
+      s_wt[e] = q < W ? es_kernel_t((T)(s_uu[kk] - (double)(s_q0[kk] + q)), ihw, beta) : (T)0;
+    }
     for (int kk = tid; kk < nk; kk += nthr) s_end[kk] = run_end(s_q0, nk, kk);
     __syncthreads();
   };

@@ -252,3 +252,22 @@ def test_launch_counter_moves(cuda):
     r, k = grids("uniform", 3000, 3000, 40)
     pn.nufht_batch(0.0, r, np.ones((3000, 2)), k)
     assert L.lib().nufht_b200_launch_count() > before
+
+
+def test_pynufht_plan_cache(cuda, orc):
+    """Repeated nufht_batch calls on the same grids reuse one cached plan; other grids or
+    tolerances get their own; results match the oracle every time."""
+    from nufht_b200 import _pynufht as pn
+    pn.clear_plan_cache()
+    r, k = grids("uniform", 2500, 2000, 21)
+    rng = np.random.default_rng(21)
+    for q in range(3):
+        c = rng.standard_normal((2500, 2))
+        g = pn.nufht_batch(0.0, r, c, k, 1e-8)
+        assert col_err(g, orc.nufht_batch(0.0, r, k, c, 1e-8), c).max() <= 1e-8
+    assert len(pn._plans.entries) == 1
+    pn.nufht_batch(0.0, r, c, k, 1e-6)
+    pn.nufht_batch(1.0, r, c, k, 1e-8)
+    assert len(pn._plans.entries) == 3
+    pn.clear_plan_cache()
+    assert not pn._plans.entries
