@@ -52,46 +52,38 @@ int launch_spread_lpt(DevicePlan& D, const AsyClass& K, const double* cs, int ld
   return launch_spread_kind<T, W, LPT, false>(D, K, K.spreadA0, K.nspreadA, cs, ld_cs, B, st);
 }
 
-template <typename T, int W, int LPT, bool SHFL>
+template <typename T, int W, int LPT>
 int launch_interp_lpt(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, int B, cudaStream_t st,
                       double sgn) {
   const AsyShape L = asy_shape(D, B, LPT);
-  size_t sm = interp_smem<T>(W, D.NLP, SHFL ? 0 : L.threads).total;
+  size_t sm = interp_smem<T>(W, D.NLP, L.threads).total;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(k_asy_interp<T, W, LPT, SHFL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         220 * 1024);
+    cudaFuncSetAttribute(k_asy_interp<T, W, LPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     attr_set = true;
   }
   dim3 g((unsigned)K.ninterp, (unsigned)L.ngy);
-  k_asy_interp<T, W, LPT, SHFL><<<g, L.threads, sm, st>>>(
-      D.d_ws, gs, ld_gs, B, (const typename Cplx<T>::type*)D.d_grid, D.d_asyb, D.d_interp + K.interp0,
-      D.d_post, K.ac, L.BT, L.V_total, sgn);
+  k_asy_interp<T, W, LPT><<<g, L.threads, sm, st>>>(D.d_ws, gs, ld_gs, B, (const typename Cplx<T>::type*)D.d_grid,
+                                                    D.d_asyb, D.d_interp + K.interp0, D.d_post, K.ac, L.BT,
+                                                    L.V_total, sgn);
   NUFHT_LAUNCH_CHECK();
   return 0;
 }
 
 // Terms per thread (register blocking): LPT = 2, or 1 in double precision for windows wider
-// than 10 (register budget); NLP = 2 (K + 1) is even.  Interpolation reduces a column's
-// partial sums with warp shuffles when its NLP / LPT threads are a power of two.
+// than 10 (register budget); NLP = 2 (K + 1) is even.
 template <typename T, int W>
 int launch_spread(DevicePlan& D, const AsyClass& K, const double* cs, int ld_cs, int B, cudaStream_t st) {
   if constexpr (sizeof(T) == 8 && W > 10) return launch_spread_lpt<T, W, 1>(D, K, cs, ld_cs, B, st);
   else return launch_spread_lpt<T, W, 2>(D, K, cs, ld_cs, B, st);
 }
 
-template <typename T, int W, int LPT>
-int launch_interp_ng(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, int B, cudaStream_t st, double sgn) {
-  const int NG = D.NLP / LPT;
-  if ((NG & (NG - 1)) == 0) return launch_interp_lpt<T, W, LPT, true>(D, K, gs, ld_gs, B, st, sgn);
-  return launch_interp_lpt<T, W, LPT, false>(D, K, gs, ld_gs, B, st, sgn);
-}
 
 template <typename T, int W>
 int launch_interp(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, int B, cudaStream_t st, double sgn) {
   if (K.ninterp == 0) return 0;
-  if constexpr (sizeof(T) == 8 && W > 10) return launch_interp_ng<T, W, 1>(D, K, gs, ld_gs, B, st, sgn);
-  else return launch_interp_ng<T, W, 2>(D, K, gs, ld_gs, B, st, sgn);
+  if constexpr (sizeof(T) == 8 && W > 10) return launch_interp_lpt<T, W, 1>(D, K, gs, ld_gs, B, st, sgn);
+  else return launch_interp_lpt<T, W, 2>(D, K, gs, ld_gs, B, st, sgn);
 }
 
 #define NUFHT_W_DISPATCH(FN, T, Wv, ...)          \

@@ -410,14 +410,14 @@ __global__ void __launch_bounds__(256) k_asy_spread(
 
 // Stage 3.  Thread (tl, g) owns terms g LPT .. g LPT + LPT - 1 of column t0 + tl.  Targets
 // are sorted, so the first cell q0 of their stencil never decreases; the CTA walks the cells
-// in order with a ring of R = W + 1 grid values per vector in registers: W for the current
-// stencil and one fetched a cell ahead, so that a load has a whole cell step to arrive.  The
-// walk is unrolled R times, which makes every ring index a compile-time constant.  Each
-// thread combines its terms with the per-target factors mu (rounded to the arithmetic type
-// from their FP64 values); the NG partial sums of a column are added with warp shuffles
-// (SHFL: NG a power of two, so a column's threads share a warp) or through shared memory,
-// then atomically into g in FP64.
-template <typename T, int W, int LPT, bool SHFL>
+// in order with a ring of R = W + 1 grid values per vector in registers (the stencil plus one
+// cell fetched a step ahead); the walk is unrolled R times, which makes every ring index a
+// compile-time constant.  Each thread combines its terms with the per-target factors mu
+// (rounded to the arithmetic type from their FP64 values) and leaves its partial sum in
+// shared memory; at the end of each chunk of targets the NG partials of a column are added
+// in FP64 and atomically into g, consecutive threads taking consecutive targets of a column.
+// (Warp shuffles for the partial sums measured slower on B200.)
+template <typename T, int W, int LPT>
 __global__ void __launch_bounds__(256) k_asy_interp(
     const double* __restrict__ ws, double* __restrict__ gs, int ld_gs, int B,
     const typename Cplx<T>::type* __restrict__ grid, const AsyBoxD* __restrict__ boxes,
@@ -436,14 +436,11 @@ __global__ void __launch_bounds__(256) k_asy_interp(
   const int tl = tid / NG, g = tid - tl * NG;
   const int t0 = blockIdx.y * BT;
   const bool active = tl < BT && t0 + tl < B;
-  // lanes of this thread's warp that exist (the block may end inside a warp)
-  const int wbase = tid & ~31;
-  const unsigned wmask = nthr - wbase >= 32 ? 0xffffffffu : ((1u << (nthr - wbase)) - 1u);
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const InterpSmem L = interp_smem<T>(W, NLP, SHFL ? 0 : nthr);
+  const InterpSmem L = interp_smem<T>(W, NLP, nthr);
   C2* s_mu = reinterpret_cast<C2*>(smem_raw + L.mu);        // [KC][NLP]
-  double* s_y = reinterpret_cast<double*>(smem_raw + L.y);  // [KC][YP] (not SHFL)
+  double* s_y = reinterpret_cast<double*>(smem_raw + L.y);  // [KC][YP]
   T* s_wt = reinterpret_cast<T*>(smem_raw + L.wt);          // [KC][WE]
   int* s_q0 = reinterpret_cast<int*>(smem_raw + L.q0);      // [KC]
   int* s_end = reinterpret_cast<int*>(smem_raw + L.end);    // [KC]: end of the equal-q0 run
@@ -455,7 +452,6 @@ __global__ void __launch_bounds__(256) k_asy_interp(
   for (int u = 0; u < LPT; ++u)
     row[u] = grid + (size_t)bx.cell_off * (size_t)V_total +
              (size_t)(active ? (t0 + tl) * NLP + g * LPT + u : 0) * (size_t)n2;
-  double* gcol = gs + (size_t)(active ? t0 + tl : 0) * ld_gs;
   const T ihw = (T)(2.0 / (double)W);
   const T beta = (T)P.beta;
   const double u_scale = bx.h * (double)n2 / (2.0 * M_PI);
@@ -494,9 +490,8 @@ __global__ void __launch_bounds__(256) k_asy_interp(
     for (int kk = tid; kk < nk; kk += nthr) s_end[kk] = run_end(s_q0, nk, kk);
     __syncthreads();
   };
-  // Shared-memory reduction of the NG partials of each column (not SHFL; all threads).
+  // Sum the NG partials of each column and add them to g (all threads).
   auto flush = [&](int k0, int nk) {
-    if (SHFL) return;
     __syncthreads();
     for (int e = tid; e < nk * BT; e += nthr) {
       int tt = e / nk, kk = e - tt * nk;
@@ -542,12 +537,7 @@ __global__ void __launch_bounds__(256) k_asy_interp(
                 y = fma(mu.x, f.x, y);
                 y = fma(-mu.y, f.y, y);
               }
-              if (SHFL) {
-                for (int off = NG >> 1; off > 0; off >>= 1) y += __shfl_xor_sync(wmask, y, off);
-                if (g == 0 && active) atomicAdd(gcol + k0 + k, sgn * (double)y);
-              } else {
-                s_y[k * YP + tid] = (double)y;
-              }
+              s_y[k * YP + tid] = (double)y;
             }
           }
           kp = e;
