@@ -35,25 +35,28 @@ __device__ __forceinline__ int miller_start(int M) {
 //   a_0 = 1,  a_k = a_{k-1} (4 nu^2 - (2k-1)^2) / (8k),
 // with cos chi, sin chi formed from sincos(x) so that the phase keeps full precision for
 // arguments up to the largest k r of the transform.
-__device__ inline void bessel_j01_large(double x, double* J0, double* J1) {
+__device__ inline void bessel_j01_large(double x, double* J0, double* J1, bool need_j1 = true) {
   double ix = 1.0 / x;
   double p0 = 1.0, q0 = 0.0, p1 = 1.0, q1 = 0.0;
   double t0 = 1.0, t1 = 1.0;
-  // 34 terms: the expansion is used for x >= 17, where the terms keep decreasing past
-  // k = 34 and the truncation error is below 2e-16 (checked against mpmath).
+  // Terms: at x >= 17 the terms keep decreasing past k = 34 and 34 of them leave a
+  // truncation error below 2e-16 (checked against mpmath); larger arguments need fewer
+  // (the k-th term a_k / x^k drops below 2e-17 by k = 19 at x = 25, 15 at 35, 12 at 50,
+  // 10 at 100).
+  const int nt = x >= 100.0 ? 10 : (x >= 50.0 ? 12 : (x >= 35.0 ? 15 : (x >= 25.0 ? 19 : 34)));
 #pragma unroll
   for (int k = 1; k <= 34; ++k) {
+    if (k > nt) break;
     const double d = (double)(2 * k - 1);
     const double inv8k = 1.0 / (8.0 * k);  // folded at compile time
-    t0 *= (0.0 - d * d) * inv8k * ix;
-    t1 *= (4.0 - d * d) * inv8k * ix;
     const double s = ((k >> 1) & 1) ? -1.0 : 1.0;  // (-1)^{floor(k/2)}
-    if (k & 1) {
-      q0 = fma(s, t0, q0);
-      q1 = fma(s, t1, q1);
-    } else {
-      p0 = fma(s, t0, p0);
-      p1 = fma(s, t1, p1);
+    t0 *= (0.0 - d * d) * inv8k * ix;
+    if (k & 1) q0 = fma(s, t0, q0);
+    else p0 = fma(s, t0, p0);
+    if (need_j1) {
+      t1 *= (4.0 - d * d) * inv8k * ix;
+      if (k & 1) q1 = fma(s, t1, q1);
+      else p1 = fma(s, t1, p1);
     }
   }
   double sn, cn;
@@ -99,7 +102,7 @@ __device__ inline void bessel_j01_small(double x, double* J0, double* J1, bool n
 __device__ inline double bessel_jn(int n, double x) {
   double a = 0.0, b = 0.0;
   if (x >= kHankelMinX) {
-    bessel_j01_large(x, &a, &b);
+    bessel_j01_large(x, &a, &b, n != 0);
   } else if (n <= 1 || x > (double)n) {
     bessel_j01_small(x, &a, &b, n != 0);
   }

@@ -200,9 +200,24 @@ void DevicePlan::build_lists() {
       eval.push_back({(int)b, i, std::min(kLocTargets, hb.i1 - i + 1)});
     locb.push_back(d);
   }
-  // ---- direct boxes: one target per thread for tall boxes, several for thin ones
+  // ---- direct boxes: one target per thread for tall boxes, several for thin ones.
+  // Asymptotic boxes with at most kThinDirect sources or targets are summed directly too:
+  // there the pairs are few (at most kThinDirect per point) while the NUFFT would still
+  // interpolate (or spread) every point for all NLP x B vectors.
   dir.clear();
-  for (const HBox& hb : dir_boxes) {
+  asy_direct.clear();
+  {
+    std::vector<HBox> kept;
+    for (const HBox& hb : asy_boxes) {
+      const int ni = hb.i1 - hb.i0 + 1, nj = hb.j1 - hb.j0 + 1;
+      if (std::min(ni, nj) <= kThinDirect) asy_direct.push_back(hb);
+      else kept.push_back(hb);
+    }
+    asy_eval = kept;
+  }
+  std::vector<HBox> all_dir = dir_boxes;
+  all_dir.insert(all_dir.end(), asy_direct.begin(), asy_direct.end());
+  for (const HBox& hb : all_dir) {
     int ni = hb.i1 - hb.i0 + 1;
     int lanes = ni >= kDirThreads ? 1 : std::min(32, kDirThreads / next_pow2(ni));
     int tpc = kDirThreads / lanes;  // targets per CTA
@@ -240,7 +255,7 @@ void DevicePlan::build_lists() {
     if (!(allowed & 4)) Wc[2] = 0;
   }
   std::vector<AsyBoxD> tmp;
-  for (const HBox& hb : asy_boxes) {
+  for (const HBox& hb : asy_eval) {
     AsyBoxD d;
     std::memset(&d, 0, sizeof(d));
     d.i0 = hb.i0;
@@ -370,8 +385,9 @@ void DevicePlan::build_lists() {
           s.l_start = l_start;
           s.ncell = ncell;
           s.fft_start = fft_start;
-          s.js = first_ge((long long)l_start - Wb);
-          s.je = first_ge((long long)l_start + ncell + 1);
+          // sources whose support [l0, l0 + W) meets the tile's cells
+          s.js = first_ge((long long)l_start - Wb + 1);
+          s.je = first_ge((long long)l_start + ncell);
           spread.push_back(s);
         };
         for (int l = 0; l <= d.half; l += kSpreadTile) add_tile(l, std::min(kSpreadTile, d.half - l + 1), l);

@@ -92,6 +92,7 @@ struct DevicePlan {
   std::vector<double> h_rs, h_ws;
   std::vector<HBox> loc_boxes, asy_boxes, dir_boxes;  // boxes as evaluated
   std::vector<HBox> plan_loc, plan_asy, plan_dir;     // the planner's partition
+  std::vector<HBox> asy_eval, asy_direct;  // asymptotic boxes evaluated by NUFFT / summed directly
 
   // work lists
   int KL1 = 0, W = 0;

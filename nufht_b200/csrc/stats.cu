@@ -34,6 +34,7 @@ void plan_stats(const DevicePlan& D, double* out, int n) {
     s[9] += 5.0 * b.n2 * std::log2((double)b.n2);
   }
   for (const HBox& b : D.dir_boxes) s[5] += (double)(b.i1 - b.i0 + 1) * (double)(b.j1 - b.j0 + 1);
+  for (const HBox& b : D.asy_direct) s[5] += (double)(b.i1 - b.i0 + 1) * (double)(b.j1 - b.j0 + 1);
   for (const HBox& b : D.loc_boxes) {
     s[6] += b.j1 - b.j0 + 1;
     s[7] += b.i1 - b.i0 + 1;
