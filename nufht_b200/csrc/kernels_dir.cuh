@@ -12,7 +12,7 @@ namespace hankel {
 constexpr int kDirThreads = 128;
 constexpr int kDirSources = 1024;  // sources per work item
 constexpr int kDirChunk = 64;      // sources staged in shared memory per round
-constexpr int kThinDirect = 4;     // asymptotic boxes this thin (sources or targets) are summed directly
+constexpr int kThinDirect = 16;    // asymptotic boxes this thin (sources or targets) are summed directly
 
 template <int BT>
 __global__ void __launch_bounds__(kDirThreads) k_dir(
