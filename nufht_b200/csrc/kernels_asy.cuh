@@ -115,7 +115,7 @@ __host__ __device__ inline InterpSmem interp_smem(int W, int NLP, int threads) {
   InterpSmem L{};
   L.mu = 0;
   L.y = align16(L.mu + (size_t)kInterpChunk * NLP * 2 * sizeof(T));
-  L.wt = align16(L.y + (threads > 0 ? (size_t)kInterpChunk * (threads + 1) * sizeof(double) : 0));
+  L.wt = align16(L.y + (size_t)kInterpChunk * (threads + 1) * sizeof(T));
   L.q0 = align16(L.wt + (size_t)kInterpChunk * interp_we<T>(W) * sizeof(T));
   L.end = align16(L.q0 + (size_t)kInterpChunk * 4);
   L.uu = align16(L.end + (size_t)kInterpChunk * 4);
@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(256) k_asy_interp(
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const InterpSmem L = interp_smem<T>(W, NLP, nthr);
   C2* s_mu = reinterpret_cast<C2*>(smem_raw + L.mu);        // [KC][NLP]
-  double* s_y = reinterpret_cast<double*>(smem_raw + L.y);  // [KC][YP]
+  T* s_y = reinterpret_cast<T*>(smem_raw + L.y);  // [KC][YP]: per-thread partial sums (already in T)
   T* s_wt = reinterpret_cast<T*>(smem_raw + L.wt);          // [KC][WE]
   int* s_q0 = reinterpret_cast<int*>(smem_raw + L.q0);      // [KC]
   int* s_end = reinterpret_cast<int*>(smem_raw + L.end);    // [KC]: end of the equal-q0 run
@@ -497,7 +497,7 @@ __global__ void __launch_bounds__(256) k_asy_interp(
       int tt = e / nk, kk = e - tt * nk;
       if (t0 + tt < B) {
         double sum = 0.0;
-        for (int q = 0; q < NG; ++q) sum += s_y[kk * YP + tt * NG + q];
+        for (int q = 0; q < NG; ++q) sum += (double)s_y[kk * YP + tt * NG + q];
         atomicAdd(&gs[(size_t)(t0 + tt) * ld_gs + k0 + kk], sgn * sum);
       }
     }
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(256) k_asy_interp(
                 y = fma(mu.x, f.x, y);
                 y = fma(-mu.y, f.y, y);
               }
-              s_y[k * YP + tid] = (double)y;
+              s_y[k * YP + tid] = y;
             }
           }
           kp = e;
