@@ -5,7 +5,14 @@ Workload: nu = 0; N = M = 1e6 sources r and targets k drawn as 1000 (1 - U[0,1))
 B = 32 columns of c ~ N(0,1) (seed 1, plus the rank); tol 1e-8.  One step = one forward
 transform on (r -> k) and one adjoint transform on (k -> r) of B columns each.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--precision fp64|mixed]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--precision mixed-averaged|mixed|fp64]
+
+Precision: mixed-averaged (default) runs the asymptotic boxes in FP32 and reports the
+forward output's error against FP64 direct sums at sampled targets beside the planner's
+worst-case FP32 bound (a column concentrated on one source); mixed keeps FP64 wherever that
+bound exceeds tol / 4 (at tol 1e-8 this workload then runs in FP64); fp64 is the plain form.
+The plain FP64 form is always timed beside a mixed one.
 
 Under torchrun each rank transforms its own B columns with the same grids (weak scaling,
 no data-path collective); the reported time is the maximum over ranks.  Rank 0 prints one
@@ -192,7 +199,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed-averaged", choices=["fp64", "mixed", "mixed-averaged"])
     ap.add_argument("--n", type=int, default=1000000)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -238,10 +245,11 @@ def main():
     from nufht_b200 import DevicePlan
     from nufht_b200 import _lib as L
     lib = L.lib()
-    mixed = args.precision == "mixed"
+    mixed_arg = {"fp64": False, "mixed": True, "mixed-averaged": "averaged"}[args.precision]
     r, k, c_h, y_h = make_inputs(N, M, B, rank)
-    pf = DevicePlan(0.0, r, k, tol, mixed=mixed, device=local)
-    pa = DevicePlan(0.0, k, r, tol, mixed=mixed, device=local)
+    pf = DevicePlan(0.0, r, k, tol, mixed=mixed_arg, device=local)
+    pa = DevicePlan(0.0, k, r, tol, mixed=mixed_arg, device=local)
+    mixed = bool(pf.info()["mixed"])  # asymptotic boxes in FP32
     c = torch.tensor(c_h, device=dev)
     y = torch.tensor(y_h, device=dev)
     g = torch.empty((B, M), dtype=torch.float64, device=dev)
@@ -279,7 +287,7 @@ def main():
 
     # The plain FP64 form of the same method on the same inputs, for the mixed/FP64 ratio.
     fp64 = None
-    if mixed:
+    if args.precision != "fp64":
         qf = DevicePlan(0.0, r, k, tol, mixed=False, device=local)
         qa = DevicePlan(0.0, k, r, tol, mixed=False, device=local)
 
@@ -319,7 +327,7 @@ def main():
     # End to end through the reference-facing C ABI: nufht_plan_init / nufht_batch with host
     # buffers (pinned), the copies inside the timed region.  The precision of that entry
     # point is chosen with NUFHT_B200_PRECISION (read when a plan first runs).
-    os.environ["NUFHT_B200_PRECISION"] = "mixed" if mixed else "fp64"
+    os.environ["NUFHT_B200_PRECISION"] = args.precision
     plans = []
     for (a, b) in ((r, k), (k, r)):
         p = L.NufhtPlan()
@@ -401,6 +409,22 @@ def main():
                             "frac": ach_tf / fp32_peak.value if fp32_peak.value > 0 else None,
                             "peak_source": "measured FP32 packed-FMA probe (nufht_b200_fp32_peak)"}
 
+    # Accuracy of this run's forward output: error against FP64 direct sums (the library's
+    # direct evaluator, every source, no expansion) at 64 sampled targets, per column over
+    # ||c_t||_1, beside the planner's worst-case bound for FP32 rounding (per ||c||_1).
+    pf.execute_columns(c, g, st)
+    torch.cuda.synchronize(dev)
+    idx = np.sort(np.random.default_rng(7).choice(M, 64, replace=False))
+    ks = np.ascontiguousarray(k[idx])
+    ex = np.zeros((64, B), order="F")
+    cF = np.asfortranarray(c_h.T)
+    lib.add_dir_batch(L.dptr(ex), 0.0, L.dptr(r), L.dptr(cF), L.dptr(ks), N, 64, B, N, 64)
+    got = g[:, torch.tensor(idx, device=dev)].cpu().numpy().T
+    err = float((np.abs(got - ex).max(axis=0) / np.abs(c_h).sum(axis=1)).max())
+    accuracy = {"max_err_over_l1": err, "over_tol": err / tol, "targets_sampled": 64,
+                "reference": "FP64 direct sums (all sources) at sampled targets of the forward transform",
+                "fp32_worst_case_bound_over_l1": float(pf.stats()[14]) if mixed else None}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         B_s = max(1, min(B, cores))
@@ -416,7 +440,7 @@ def main():
                 "data": "synthetic (seeded numpy draws with the workload's shapes)", "config": config,
                 "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches),
                 "phases_ms_per_step": phases, "roofline": roofline, "cpu_baseline": cpu,
-                "fp64_form": fp64, "plan": pf.info()}
+                "fp64_form": fp64, "accuracy": accuracy, "plan": pf.info()}
         print(json.dumps(line))
     pf.close()
     pa.close()

@@ -165,7 +165,15 @@ void add_loc_batch(double *gs, double nu, const double *rs, const double *cs,
 
 /* Plan flags. */
 #define NUFHT_B200_FP64            0x0   /* all arithmetic in FP64 (default) */
-#define NUFHT_B200_MIXED           0x1   /* mixed precision (FP32 storage / split products) */
+#define NUFHT_B200_MIXED           0x1   /* asymptotic boxes in FP32 where the modelled worst-case
+                                            FP32 error is at most tol / 4 (plan info: mixed = 1),
+                                            FP64 otherwise */
+#define NUFHT_B200_MIXED_AVERAGED  0x2   /* asymptotic boxes in FP32 for tol >= 1e-9 whatever the
+                                            worst case: within tol for coefficient columns spread
+                                            over many sources (their FP32 rounding averages out;
+                                            measured against FP64 direct sums), up to the
+                                            plan_stats bound out[14] * ||c||_1 for a column
+                                            concentrated on one source */
 #define NUFHT_B200_EXTENDED_TABLES 0x10  /* fill the asymptotic table at K_asy = 10, which the
                                             reference leaves empty (affects |nu| >= 35) */
 
@@ -223,9 +231,12 @@ void nufht_b200_set_phase_timing(int on);
 int nufht_b200_phase_times(double *ms, int nphase);
 
 /* Algorithmic work of a plan, per batch column where it scales with the batch:
- * out[0..11] = asymptotic sources, asymptotic targets, FFT cells, spreading taps,
+ * out[0..14] = asymptotic sources, asymptotic targets, FFT cells, spreading taps,
  * interpolation taps, direct pairs, local sources, local targets, FFT cells read by
- * interpolation, FFT flops per vector, expansion terms (2 (K_asy + 1)), K_loc + 1. */
+ * interpolation, FFT flops per vector, expansion terms (2 (K_asy + 1)), K_loc + 1,
+ * asymptotic boxes oversampled below 2, 1 if the asymptotic boxes run in FP32 (mixed
+ * precision) else 0, and the modelled worst-case error of FP32 asymptotic boxes per unit
+ * ||c||_1 (mixed precision is used only where it is at most tol / 4). */
 int nufht_b200_plan_stats(const NufhtDevicePlan *plan, double *out, int n);
 
 /* Measured FP64 fused-multiply-add throughput of the current device (TFLOP/s). */

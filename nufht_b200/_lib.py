@@ -57,6 +57,7 @@ class NufhtB200Info(ctypes.Structure):
 
 NUFHT_B200_FP64 = 0x0
 NUFHT_B200_MIXED = 0x1
+NUFHT_B200_MIXED_AVERAGED = 0x2
 NUFHT_B200_EXTENDED_TABLES = 0x10
 NUFHT_E_UNSORTED_RS = -410
 NUFHT_E_UNSORTED_WS = -411

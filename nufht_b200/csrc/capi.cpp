@@ -189,9 +189,12 @@ int device_state_for(const NufhtPlan* plan, DevicePlan** out) {
   D->plan_asy = to_hbox(plan->boxes.asy);
   D->plan_dir = to_hbox(plan->boxes.dir);
   // The reference's entry points carry no precision argument; NUFHT_B200_PRECISION=mixed
-  // selects the mixed-precision asymptotic path for them (same rule as NUFHT_B200_MIXED).
-  if (const char* pr = std::getenv("NUFHT_B200_PRECISION"))
-    D->mixed_asy = std::strcmp(pr, "mixed") == 0 && D->P.tol >= 1e-9;
+  // or mixed-averaged selects the mixed-precision asymptotic path for them (the rules of
+  // NUFHT_B200_MIXED and NUFHT_B200_MIXED_AVERAGED).
+  if (const char* pr = std::getenv("NUFHT_B200_PRECISION")) {
+    D->mixed_averaged = std::strcmp(pr, "mixed-averaged") == 0;
+    D->mixed_asy = (std::strcmp(pr, "mixed") == 0 || D->mixed_averaged) && D->P.tol >= 1e-9;
+  }
   choose_path(D.get(), plan->min_dim_prod);
   int dev = 0;
   cudaGetDevice(&dev);
@@ -558,7 +561,7 @@ int nufht_b200_plan_create(NufhtDevicePlan** out, double nu, const double* rs, i
   if (!out) return -200;
   *out = nullptr;
   if (!rs || !ws || m <= 0 || n <= 0) return -200;
-  if (flags & ~(NUFHT_B200_MIXED | NUFHT_B200_EXTENDED_TABLES)) return NUFHT_E_BAD_FLAGS;
+  if (flags & ~(NUFHT_B200_MIXED | NUFHT_B200_MIXED_AVERAGED | NUFHT_B200_EXTENDED_TABLES)) return NUFHT_E_BAD_FLAGS;
   NufhtOptions opt = opt_in ? *opt_in : nufht_default_options();
   std::unique_ptr<DevicePlan> D(new DevicePlan);
   int rc = hankel::fill_params(nu, opt, (flags & NUFHT_B200_EXTENDED_TABLES) != 0, &D->P);
@@ -568,9 +571,11 @@ int nufht_b200_plan_create(NufhtDevicePlan** out, double nu, const double* rs, i
   D->m = m;
   D->n = n;
   D->flags = flags;
-  // Mixed precision: the asymptotic boxes (the bulk of the work) run in FP32; below
-  // tol = 1e-9 single precision cannot reach the requested accuracy and FP64 is kept.
-  D->mixed_asy = (flags & NUFHT_B200_MIXED) != 0 && D->P.tol >= 1e-9;
+  // Mixed precision requested: the asymptotic boxes (the bulk of the work) run in FP32 if
+  // the planner finds the worst-case FP32 rounding within tol / 4 (NUFHT_B200_MIXED) or
+  // regardless of it (NUFHT_B200_MIXED_AVERAGED), else in FP64; always FP64 below 1e-9.
+  D->mixed_asy = (flags & (NUFHT_B200_MIXED | NUFHT_B200_MIXED_AVERAGED)) != 0 && D->P.tol >= 1e-9;
+  D->mixed_averaged = (flags & NUFHT_B200_MIXED_AVERAGED) != 0;
   if ((rc = host_copy(rs, m, &D->h_rs)) || (rc = host_copy(ws, n, &D->h_ws))) return rc;
   if (hankel::check_grid(D->h_rs.data(), m)) return NUFHT_E_UNSORTED_RS;
   if (hankel::check_grid(D->h_ws.data(), n)) return NUFHT_E_UNSORTED_WS;

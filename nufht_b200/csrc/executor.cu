@@ -110,6 +110,36 @@ int next_pow2(int v) {
 // grid and the FFT (memory-bound boxes with few points per cell).
 const double kSigmas[3] = {2.0, 1.5, 1.25};
 
+// psi-hat(0) / psi-hat(pi / sigma) for the three oversampling classes: the factor by which
+// deconvolution amplifies rounding at the edge of the band.
+const double kKappa[3] = {3.0, 26.0, 1100.0};
+
+// Worst-case error of the asymptotic boxes in FP32 arithmetic, per unit ||c||_1 (all of c
+// on one source), for deconvolution amplification kappa.  Every FP32 stage rounds relative
+// to the magnitude of the expansion term it carries, and term lp of a box is at most
+// |coef_lp| x^-(lp+1/2) per unit |c_j| with x = k r >= k_lo rref over the box, so
+//   err = max over boxes of  kFp32Err kappa sum_lp sqrt(2/pi) |a_lp| x_min^-(lp+1/2),
+// kFp32Err fitted to single-source columns on B200 (the measured error stayed below 0.9 of
+// the model over orders 0 to 25, half-integer orders and tolerances 1e-6 to 1e-8).
+double fp32_error_bound(const DevicePlan& D, double kappa) {
+  constexpr double kFp32Err = 5e-7;
+  const int NLP = 2 * (D.P.K_asy + 1);
+  const double s2p = std::sqrt(2.0 / M_PI);
+  const double* rs = D.h_rs.data();
+  const double* ws = D.h_ws.data();
+  double err = 0.0;
+  for (const HBox& hb : D.asy_eval) {
+    const double* p = std::upper_bound(rs + hb.j0, rs + hb.j1 + 1, 0.0);
+    if (p > rs + hb.j1) continue;  // only sources at r = 0: nothing to evaluate
+    const double x = ws[hb.i0] * *p;
+    if (!(x > 0.0)) continue;
+    double sum = 0.0;
+    for (int lp = 0; lp < NLP && lp < 64; ++lp) sum += s2p * std::fabs(D.P.asy_coef[lp]) * std::pow(x, -(lp + 0.5));
+    err = std::max(err, kFp32Err * kappa * sum);
+  }
+  return err;
+}
+
 // Kernel shape for oversampling sigma and width W: beta = 2.30 W at sigma = 2 (the
 // value of Barnett, Magland & af Klinteberg 2019), 0.97 pi (1 - 1/(2 sigma)) W otherwise.
 double es_beta(double sigma, int W) {
@@ -240,8 +270,11 @@ void DevicePlan::build_lists() {
   for (int c = 0; c < 3; ++c) Wc[c] = spread_width(P.tol, kSigmas[c]);
   // In FP32 the deconvolution by psi-hat amplifies rounding by psi-hat(0)/psi-hat(pi/sigma):
   // about 3 at sigma = 2, 26 at 1.5 and 1100 at 1.25, so mixed precision keeps sigma = 2
-  // unless NUFHT_B200_MIXED_SIGMAS lists the classes to allow (tuning: "2,1.5").
-  if (mixed_asy) {
+  // unless NUFHT_B200_MIXED_SIGMAS lists the classes to allow (tuning: "2,1.5").  It runs
+  // only where the modelled worst case of FP32 rounding stays within a quarter of the
+  // tolerance (other plans evaluate their asymptotic boxes in FP64), unless the caller
+  // accepts rounding that averages out over many sources (mixed_averaged).
+  {
     static const int allowed = [] {
       const char* e = std::getenv("NUFHT_B200_MIXED_SIGMAS");
       int mask = 1;
@@ -251,8 +284,13 @@ void DevicePlan::build_lists() {
       }
       return mask;
     }();
-    if (!(allowed & 2)) Wc[1] = 0;
-    if (!(allowed & 4)) Wc[2] = 0;
+    const double kappa = (allowed & 4) ? kKappa[2] : (allowed & 2) ? kKappa[1] : kKappa[0];
+    fp32_err = fp32_error_bound(*this, kappa);
+    if (mixed_asy && !mixed_averaged && fp32_err > 0.25 * P.tol) mixed_asy = false;
+    if (mixed_asy) {
+      if (!(allowed & 2)) Wc[1] = 0;
+      if (!(allowed & 4)) Wc[2] = 0;
+    }
   }
   std::vector<AsyBoxD> tmp;
   for (const HBox& hb : asy_eval) {

@@ -129,7 +129,9 @@ struct DevicePlan {
   size_t fft_work_bytes = 0;
   size_t ws_bytes = 0;
   void* d_grid = nullptr;    // complex FP64 (double2) or, in mixed precision, FP32 (float2)
-  bool mixed_asy = false;    // asymptotic boxes in FP32 (set for NUFHT_B200_MIXED, tol >= 1e-9)
+  bool mixed_asy = false;    // asymptotic boxes in FP32 (NUFHT_B200_MIXED, where FP32 meets tol)
+  bool mixed_averaged = false;  // FP32 regardless of the worst-case bound (NUFHT_B200_MIXED_AVERAGED)
+  double fp32_err = 0.0;     // modelled worst-case FP32 error of the asymptotic boxes per ||c||_1
   double* d_partial = nullptr;
   double* d_cheb = nullptr;
   void* d_fft_work = nullptr;

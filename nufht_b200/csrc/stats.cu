@@ -20,8 +20,11 @@ namespace hankel {
 // out[9]  FFT flops per vector (sum of 5 n2 log2 n2)
 // out[10] expansion terms per column (NLP)
 // out[11] local expansion terms (K_loc + 1)
+// out[12] asymptotic boxes oversampled below sigma = 2
+// out[13] 1 if the asymptotic boxes run in FP32 (mixed precision), else 0
+// out[14] modelled worst-case error of the asymptotic boxes in FP32, per unit ||c||_1
 void plan_stats(const DevicePlan& D, double* out, int n) {
-  double s[12] = {0};
+  double s[15] = {0};
   for (const AsyBoxD& b : D.asyb) {
     double nj = b.j1 - b.j0 + 1, ni = b.i1 - b.i0 + 1;
     const AsyClass& K = D.classes[b.cls];
@@ -32,6 +35,7 @@ void plan_stats(const DevicePlan& D, double* out, int n) {
     s[4] += ni * K.W;
     s[8] += std::min((double)b.n2, b.n2 / K.sigma + K.W);
     s[9] += 5.0 * b.n2 * std::log2((double)b.n2);
+    if (K.sigma != 2.0) s[12] += 1.0;
   }
   for (const HBox& b : D.dir_boxes) s[5] += (double)(b.i1 - b.i0 + 1) * (double)(b.j1 - b.j0 + 1);
   for (const HBox& b : D.asy_direct) s[5] += (double)(b.i1 - b.i0 + 1) * (double)(b.j1 - b.j0 + 1);
@@ -41,7 +45,9 @@ void plan_stats(const DevicePlan& D, double* out, int n) {
   }
   s[10] = D.NLP;
   s[11] = D.KL1;
-  for (int i = 0; i < n && i < 12; ++i) out[i] = s[i];
+  s[13] = D.mixed_asy ? 1.0 : 0.0;
+  s[14] = D.fp32_err;
+  for (int i = 0; i < n && i < 15; ++i) out[i] = s[i];
 }
 
 namespace {

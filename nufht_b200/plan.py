@@ -23,6 +23,12 @@ class DevicePlan:
     r (m sources) and k (n targets) must be finite, non-negative and non-decreasing.
     Planning (box partition, work lists, FFT plans) happens once; each call runs the
     transform on the current torch stream.
+
+    mixed: False (FP64), True (asymptotic boxes in FP32 where the planner's worst-case FP32
+    error bound is within tol / 4, FP64 elsewhere) or "averaged" (FP32 for tol >= 1e-9
+    regardless of that bound: within tol when each column's mass is spread over many
+    sources, up to stats()[14] * ||c||_1 for a column concentrated on one source).
+    info()["mixed"] says whether the asymptotic boxes run in FP32.
     """
 
     def __init__(self, nu, r, k, tol=1e-8, *, mixed=False, extended_tables=False, device=None,
@@ -36,7 +42,10 @@ class DevicePlan:
         if device is None:
             device = torch.cuda.current_device()
         self.device = torch.device("cuda", int(device) if not isinstance(device, torch.device) else device.index or 0)
-        flags = (L.NUFHT_B200_MIXED if mixed else 0) | (L.NUFHT_B200_EXTENDED_TABLES if extended_tables else 0)
+        if mixed not in (False, True, "averaged"):
+            raise ValueError("mixed must be False, True or 'averaged'")
+        flags = ((L.NUFHT_B200_MIXED_AVERAGED if mixed == "averaged" else L.NUFHT_B200_MIXED if mixed else 0)
+                 | (L.NUFHT_B200_EXTENDED_TABLES if extended_tables else 0))
         opt = L.options(tol=self.tol, max_levels=max_levels, min_dim_prod=min_dim_prod, z_split=z_split,
                         K_asy=K_asy, K_loc=K_loc)
         h = ctypes.c_void_p()
@@ -45,7 +54,13 @@ class DevicePlan:
         if rc != 0:
             raise RuntimeError("nufht_b200_plan_create failed (%d): %s" % (rc, L.strerror(rc)))
         self._h = h
-        self.mixed = bool(mixed)
+        self.mixed = mixed
+
+    def stats(self):
+        """Work counts of the plan and its FP32 error model (nufht_b200_plan_stats, 15 values)."""
+        st = np.zeros(15)
+        L.lib().nufht_b200_plan_stats(self._h, st.ctypes.data_as(L.c_double_p), 15)
+        return st
 
     def info(self):
         inf = L.NufhtB200Info()

@@ -29,7 +29,7 @@ class HankelPlans:
     same r and k plan once."""
 
     def __init__(self, nu, r, k, tol=1e-8, mixed=False, extended_tables=False):
-        self.nu, self.tol, self.mixed = float(nu), float(tol), bool(mixed)
+        self.nu, self.tol, self.mixed = float(nu), float(tol), mixed
         self.r = r.detach().to(torch.float64)
         self.k = k.detach().to(torch.float64)
         self.extended = bool(extended_tables)
@@ -99,7 +99,7 @@ class NufhtFunction(torch.autograd.Function):
 def nufht(c, r, k, nu, tol=1e-8, mixed=False, plans=None):
     """Differentiable g = H c.  c: (m,) or (m, B); r: (m,), k: (n,) sorted, on one GPU.
 
-    Gradients flow to c, r and k.  Pass `plans` (a HankelPlans for the same grids) to reuse
+    mixed: False, True or "averaged", as for DevicePlan.  Gradients flow to c, r and k.  Pass `plans` (a HankelPlans for the same grids) to reuse
     planning across calls with the same r and k."""
     squeeze = c.dim() == 1
     c2 = c.reshape(c.shape[0], -1).to(torch.float64)
@@ -119,7 +119,7 @@ class HankelTransform(torch.nn.Module):
 
     def __init__(self, nu, tol=1e-8, mixed=False, extended_tables=False):
         super().__init__()
-        self.nu, self.tol, self.mixed = float(nu), float(tol), bool(mixed)
+        self.nu, self.tol, self.mixed = float(nu), float(tol), mixed
         self.extended = bool(extended_tables)
         self._plans = None
         self._key = None
