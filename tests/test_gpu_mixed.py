@@ -152,3 +152,34 @@ def test_reference_entry_point_precision_switch(cuda, orc):
         finally:
             del os.environ["NUFHT_B200_PRECISION"]
         assert col_err(g, orc.nufht_batch(0.0, r, k, c, tol), c).max() <= tol
+
+
+@pytest.mark.parametrize("tol", [1e-6, 1e-10])
+def test_cfg2_full_size_tolerances(cuda, orc, tol):
+    """N = M = 1e6 on (0, 1000], batch 32 of N(0,1), tol 1e-6 and 1e-10: the plain FP64 form
+    and both mixed forms against FP64 direct sums (every source, no expansion; the library's
+    direct evaluator) at 2000 sampled targets."""
+    import torch
+    from nufht_b200 import DevicePlan
+    from nufht_b200 import _lib as L
+    N, B = 1_000_000, 32
+    rng = np.random.default_rng(1)
+    r = np.sort(1000.0 * (1.0 - rng.random(N)))
+    k = np.sort(1000.0 * (1.0 - rng.random(N)))
+    c = np.random.default_rng(2).standard_normal((N, B))
+    idx = np.sort(np.random.default_rng(3).choice(N, 2000, replace=False))
+    ks = np.ascontiguousarray(k[idx])
+    ex = np.zeros((2000, B), order="F")
+    cf = np.asfortranarray(c)
+    L.lib().add_dir_batch(L.dptr(ex), 0.0, L.dptr(r), L.dptr(cf), L.dptr(ks), N, 2000, B, N, 2000)
+    ct = torch.tensor(c, device=cuda)
+    it = torch.tensor(idx, device=cuda)
+    for mixed in (False, True, "averaged"):
+        p = DevicePlan(0.0, r, k, tol, mixed=mixed)
+        # FP32 only where allowed: never below 1e-9; strict mode only within its bound
+        expect = int(tol >= 1e-9 and (mixed == "averaged" or (mixed is True and p.stats()[14] <= 0.25 * tol)))
+        assert p.info()["mixed"] == expect
+        g = p(ct)[it].cpu().numpy()
+        err = col_err(g, ex, c)
+        assert err.max() <= tol, (mixed, tol, err.max())
+        p.close()
