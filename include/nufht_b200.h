@@ -268,6 +268,17 @@ int nufht_b200_add_loc_batch_noalloc(double *gs, double nu, const double *rs, co
  * batch (the graph records them); g is overwritten.  Creation runs every item once and
  * sizes all workspaces, so a launch allocates nothing.  The plans must not be executed
  * elsewhere while a launch of the batch is in flight. */
+/* Replaces the copies around nufht_batch in src/_pynufht.c:156,222-237 (the forced
+ * Fortran-order copy of cs and the transpose copy of g).  nufht_batch with a choice of
+ * layout for cs and gs: layout 0 = column-major as nufht_batch (column t at p + t * ld,
+ * ld >= m or n), 1 = row-major (row j at p + j * ld, ld >= batch: a C-order (m, batch)
+ * NumPy array).  Host or device pointers; synchronous.  Row-major batches are transposed
+ * on the GPU after / before one contiguous copy, so no host-side copy is made; with both
+ * layouts 0 this is nufht_batch.  Returns 0, -400 (null pointer, batch <= 0, layout not
+ * 0 or 1), -401 (leading dimension too small), or a plan / CUDA error code. */
+int nufht_b200_batch_layout(const NufhtPlan *plan, const double *cs, int c_rowmajor, int ld_cs,
+                            double *gs, int g_rowmajor, int ld_gs, int batch);
+
 typedef struct NufhtB200Batch NufhtB200Batch;
 typedef struct {
     NufhtDevicePlan *plan;

@@ -92,6 +92,8 @@ def _declare(lib):
                                        ctypes.c_int, ctypes.POINTER(NufhtScratch)]),
         "nufht_inplace": (None, [vp, ctypes.c_double, vp, ctypes.c_int, vp, vp, ctypes.c_int,
                                  ctypes.POINTER(NufhtOptions)]),
+        "nufht_b200_batch_layout": (ctypes.c_int, [ctypes.POINTER(NufhtPlan), vp, ctypes.c_int, ctypes.c_int, vp,
+                                                   ctypes.c_int, ctypes.c_int, ctypes.c_int]),
         "nufht": (vp, [ctypes.c_double, vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.POINTER(NufhtOptions)]),
         "generate_tables": (None, []),
         "add_dir": (None, [vp, ctypes.c_double, vp, vp, vp, ctypes.c_int, ctypes.c_int]),

@@ -108,19 +108,30 @@ def clear_plan_cache():
 
 
 def nufht_batch(nu, rs, cs, ws, tol=1e-8):
-    """Batched transform through nufht_plan_init / nufht_batch (src/_pynufht.c:144-239)."""
+    """Batched transform through nufht_plan_init / nufht_batch (src/_pynufht.c:144-239).
+
+    Same arguments, C-order (n, batch) result and exceptions as the reference.  The reference
+    copies cs to Fortran order and transposes g back on the host (src/_pynufht.c:156,
+    222-237); here C-order or Fortran-order cs is read as it is and the C-order result is
+    written directly (nufht_b200_batch_layout transposes on the GPU)."""
     lib = L.lib()
     rs = _vec(rs)
     ws = _vec(ws)
     cs = _check_batch(rs, cs)
-    cs = np.asfortranarray(cs)  # column-major, as the reference forces (src/_pynufht.c:156)
     m, n, batch = rs.shape[0], ws.shape[0], cs.shape[1]
+    if cs.flags.c_contiguous:
+        c_row, ld_cs = 1, batch
+    elif cs.flags.f_contiguous:
+        c_row, ld_cs = 0, m
+    else:
+        cs = np.ascontiguousarray(cs)
+        c_row, ld_cs = 1, batch
     plan = _plans.get(nu, tol, rs, ws)
-    gs = np.empty((n, batch), dtype=np.float64, order="F")
-    ret = lib.nufht_batch(ctypes.byref(plan), L.dptr(cs), m, L.dptr(gs), n, batch, None)
+    gs = np.empty((n, batch), dtype=np.float64)  # C order, as the reference returns
+    ret = lib.nufht_b200_batch_layout(ctypes.byref(plan), L.dptr(cs), c_row, ld_cs, L.dptr(gs), 1, batch, batch)
     if ret != 0:
         raise RuntimeError("nufht_batch returned %d" % ret)
-    return np.ascontiguousarray(gs)  # C-order (n, batch) result (src/_pynufht.c:222-237)
+    return gs
 
 
 def nufht_batch_loop(nu, rs, cs, ws, tol=1e-8):

@@ -2,6 +2,7 @@
 // backed by the GPU executor, and this library's device-plan extension.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -314,6 +315,65 @@ int run_any(DevicePlan* D, const double* cs, int ld_cs, double* gs, int ld_gs, i
   return 0;
 }
 
+// nufht_batch with either layout of cs and gs (column-major with leading dimension ld, or
+// row-major with row pitch ld >= B), host or device pointers, synchronous.  Row-major
+// batches are transposed on the GPU (one contiguous host copy each way, no host-side
+// transposes); the transform itself runs on column-major device buffers in one block.
+int run_layout(DevicePlan* D, const double* cs, bool crow, int ld_cs, double* gs, bool grow, int ld_gs, int B) {
+  std::lock_guard<std::mutex> lk(D->mu);
+  if (cudaSetDevice(D->device) != cudaSuccess) return NUFHT_E_CUDA;
+  cudaStream_t st = 0;
+  const bool cdev = is_device_ptr(cs), gdev = is_device_ptr(gs);
+  const size_t m = (size_t)D->m, n = (size_t)D->n;
+  int rc;
+  const bool need_t = (crow && !cdev) || (grow && !gdev);
+  if ((rc = stage_buffer(&D->d_stage_c, &D->stage_c_bytes, (cdev && !crow) ? 0 : sizeof(double) * m * B)) ||
+      (rc = stage_buffer(&D->d_stage_g, &D->stage_g_bytes, (gdev && !grow) ? 0 : sizeof(double) * n * B)) ||
+      (rc = stage_buffer(&D->d_stage_t, &D->stage_t_bytes, need_t ? sizeof(double) * std::max(m, n) * B : 0)))
+    return rc;
+  // c -> column-major device matrix dc (leading dimension ldc)
+  const double* dc = cs;
+  int ldc = ld_cs;
+  if (crow) {
+    const double* src = cs;
+    int lds = ld_cs;
+    if (!cdev) {
+      if (cudaMemcpy2DAsync(D->d_stage_t, sizeof(double) * B, cs, sizeof(double) * (size_t)ld_cs, sizeof(double) * B,
+                            m, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return NUFHT_E_CUDA;
+      src = D->d_stage_t;
+      lds = B;
+    }
+    if ((rc = hankel::transpose_f64(src, lds, D->d_stage_c, D->m, D->m, B, st))) return rc;
+    dc = D->d_stage_c;
+    ldc = D->m;
+  } else if (!cdev) {
+    if (cudaMemcpy2DAsync(D->d_stage_c, sizeof(double) * m, cs, sizeof(double) * (size_t)ld_cs, sizeof(double) * m,
+                          B, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return NUFHT_E_CUDA;
+    dc = D->d_stage_c;
+    ldc = D->m;
+  }
+  // transform into a column-major device matrix dg
+  double* dg = (gdev && !grow) ? gs : D->d_stage_g;
+  const int ldg = (gdev && !grow) ? ld_gs : D->n;
+  if ((rc = D->run(dc, ldc, dg, ldg, B, st, true))) return rc;
+  // dg -> gs
+  if (grow) {
+    double* dst = gdev ? gs : D->d_stage_t;
+    const int ldd = gdev ? ld_gs : B;
+    if ((rc = hankel::transpose_f64(dg, ldg, dst, ldd, B, D->n, st))) return rc;
+    if (!gdev && cudaMemcpy2DAsync(gs, sizeof(double) * (size_t)ld_gs, D->d_stage_t, sizeof(double) * B,
+                                   sizeof(double) * B, n, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      return NUFHT_E_CUDA;
+  } else if (!gdev) {
+    if (cudaMemcpy2DAsync(gs, sizeof(double) * (size_t)ld_gs, dg, sizeof(double) * n, sizeof(double) * n, B,
+                          cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      return NUFHT_E_CUDA;
+  }
+  return cudaStreamSynchronize(st) == cudaSuccess ? 0 : NUFHT_E_CUDA;
+}
+
 // One-box evaluator for the add_* entry points.
 void run_single_box(int kind, double* gs, double nu, const double* rs, const double* cs,
                     const double* ws, int m, int n, int K, double tol, const double* asy_coef,
@@ -485,6 +545,21 @@ int nufht_batch(const NufhtPlan* plan, const double* cs, int ld_cs, double* gs, 
   }
   rc = run_any(D, cs, ld_cs, gs, ld_gs, batch, true);
   if (rc) std::fprintf(stderr, "nufht_batch: %s\n", nufht_b200_strerror(rc));
+  return rc;
+}
+
+extern "C" int nufht_b200_batch_layout(const NufhtPlan* plan, const double* cs, int c_rowmajor, int ld_cs,
+                                       double* gs, int g_rowmajor, int ld_gs, int batch) {
+  if (!plan || !cs || !gs || batch <= 0) return -400;
+  if ((c_rowmajor != 0 && c_rowmajor != 1) || (g_rowmajor != 0 && g_rowmajor != 1)) return -400;
+  if (ld_cs < (c_rowmajor ? batch : plan->m) || ld_gs < (g_rowmajor ? batch : plan->n)) return -401;
+  DevicePlan* D = nullptr;
+  int rc = device_state_for(plan, &D);
+  if (!rc) {
+    rc = (c_rowmajor || g_rowmajor) ? run_layout(D, cs, c_rowmajor != 0, ld_cs, gs, g_rowmajor != 0, ld_gs, batch)
+                                    : run_any(D, cs, ld_cs, gs, ld_gs, batch, true);
+  }
+  if (rc) std::fprintf(stderr, "nufht_b200_batch_layout: %s\n", nufht_b200_strerror(rc));
   return rc;
 }
 

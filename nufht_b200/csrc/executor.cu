@@ -522,7 +522,7 @@ DevicePlan::~DevicePlan() {
   cudaFree(d_dir); cudaFree(d_asyb); cudaFree(d_spread); cudaFree(d_interp);
   cudaFree(d_corr); cudaFree(d_post);
   cudaFree(d_grid); cudaFree(d_partial); cudaFree(d_cheb); cudaFree(d_fft_work);
-  cudaFree(d_stage_c); cudaFree(d_stage_g);
+  cudaFree(d_stage_c); cudaFree(d_stage_g); cudaFree(d_stage_t);
   if (copy_in) cudaStreamDestroy(copy_in);
   if (copy_out) cudaStreamDestroy(copy_out);
   for (int q = 0; q < 4; ++q) {

@@ -139,7 +139,8 @@ struct DevicePlan {
   // staging for host-pointer calls through the reference-compatible entry points
   double* d_stage_c = nullptr;
   double* d_stage_g = nullptr;
-  size_t stage_c_bytes = 0, stage_g_bytes = 0;
+  double* d_stage_t = nullptr;  // row-major copies of cs / gs (nufht_b200_batch_layout)
+  size_t stage_c_bytes = 0, stage_g_bytes = 0, stage_t_bytes = 0;
   // copy streams and events of the pipelined host-buffer path (created on first use)
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   cudaEvent_t ev_in[4] = {}, ev_done[4] = {};
@@ -192,6 +193,10 @@ int run_asy_f64(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_g
                 double sgn);
 
 int run_besselj(double nu, const double* x, double* out, long count, cudaStream_t st);
+
+// out[c * ldo + r] = in[r * ldi + c] for r < rows, c < cols (device pointers): a row-major
+// batch to the executor's column-major one and back.
+int transpose_f64(const double* in, int ldi, double* out, int ldo, int rows, int cols, cudaStream_t st);
 
 }  // namespace hankel
 

@@ -161,6 +161,49 @@ def test_leading_dimensions_and_device_pointers(cuda, orc):
     lib.nufht_plan_free(ctypes.byref(plan))
 
 
+def test_batch_layouts(cuda, orc):
+    """nufht_b200_batch_layout: every combination of row-major (C-order) and column-major cs
+    and gs, with padded leading dimensions, host and device pointers, against the oracle;
+    _pynufht.nufht_batch on C-order, Fortran-order and strided cs gives a C-order result."""
+    import torch
+    from nufht_b200 import _lib as L
+    from nufht_b200 import _pynufht as pn
+    lib = L.lib()
+    r, k = grids("uniform", 3000, 2000, 22)
+    m, n, B = 3000, 2000, 5
+    c = np.random.default_rng(3).standard_normal((m, B))
+    g_or = orc.nufht_batch(0.0, r, k, c, 1e-8)
+    plan = L.NufhtPlan()
+    assert lib.nufht_plan_init(ctypes.byref(plan), 0.0, L.dptr(r), m, L.dptr(k), n, None) == 0
+    for c_row in (0, 1):
+        for g_row in (0, 1):
+            ldc = (B + 3) if c_row else (m + 7)
+            ldg = (B + 2) if g_row else (n + 5)
+            cbuf = np.full((m, ldc) if c_row else (ldc, B), 123.0, order="C" if c_row else "F")
+            cbuf[:m, :B] = c
+            gbuf = np.full((n, ldg) if g_row else (ldg, B), 77.0, order="C" if g_row else "F")
+            assert lib.nufht_b200_batch_layout(ctypes.byref(plan), L.dptr(cbuf), c_row, ldc, L.dptr(gbuf), g_row,
+                                               ldg, B) == 0
+            assert col_err(gbuf[:n, :B], g_or, c).max() <= 1e-8, (c_row, g_row)
+            assert np.all(gbuf[n:] == 77.0) and np.all(gbuf[:, B:] == 77.0)  # padding untouched
+            # device pointers
+            cd = torch.tensor(np.ascontiguousarray(cbuf if c_row else cbuf.T), device=cuda)
+            gd = torch.full((n, ldg) if g_row else (B, ldg), 77.0, dtype=torch.float64, device=cuda)
+            assert lib.nufht_b200_batch_layout(ctypes.byref(plan), ctypes.c_void_p(cd.data_ptr()), c_row, ldc,
+                                               ctypes.c_void_p(gd.data_ptr()), g_row, ldg, B) == 0
+            torch.cuda.synchronize()
+            gh = gd.cpu().numpy()
+            gh = gh[:n, :B] if g_row else gh.T[:n, :B]
+            assert np.abs(gh - gbuf[:n, :B]).max() <= 1e-12 * np.abs(c).sum(axis=0).max()
+    assert lib.nufht_b200_batch_layout(ctypes.byref(plan), L.dptr(c), 2, B, L.dptr(g_or), 1, B, B) == -400
+    assert lib.nufht_b200_batch_layout(ctypes.byref(plan), L.dptr(c), 1, B - 1, L.dptr(g_or), 1, B, B) == -401
+    lib.nufht_plan_free(ctypes.byref(plan))
+    for cs in (np.ascontiguousarray(c), np.asfortranarray(c), np.ascontiguousarray(np.repeat(c, 2, axis=1))[:, ::2]):
+        g = pn.nufht_batch(0.0, r, cs, k, 1e-8)
+        assert g.flags.c_contiguous and g.shape == (n, B)
+        assert col_err(g, g_or, c).max() <= 1e-8
+
+
 def test_device_plan_torch(cuda, orc):
     import torch
     from nufht_b200 import DevicePlan
