@@ -646,7 +646,9 @@ int launch_loc(const double* rs, const double* ws, const double* cs, int ld_cs, 
   const int LS = kLocThreads / BT;
   const int NL = (KL1 + LS - 1) / LS;
   if (NL > kLocMaxNL) return NUFHT_E_TOO_LARGE;
-  const int chunk = (int)std::min<size_t>(kLocChunk, kLocSmemDoubles / (size_t)(KL1 + BT));
+  // sources per staging round: even (the projection reads the table in 16-byte pairs)
+  const int chunk = (int)std::min<size_t>(kLocChunk, kLocSmemDoubles / (size_t)(KL1 + BT)) & ~1;
+  if (chunk < 2) return NUFHT_E_TOO_LARGE;
   const size_t sm = sizeof(double) * ((size_t)KL1 * chunk + (size_t)chunk * BT);
   dim3 g((unsigned)nproj, (unsigned)((B + BT - 1) / BT));
   {

@@ -14,13 +14,19 @@ constexpr int kLocSources = 2048;  // sources per projection work item
 constexpr int kLocChunk = 64;      // sources staged per round, at most
 constexpr int kLocTargets = 128;   // targets per evaluation CTA
 constexpr int kLocThreads = 256;   // threads of a projection CTA
-constexpr int kLocMaxNL = 16;      // expansion orders per projection thread, at most
+constexpr int kLocMaxNL = 40;      // expansion orders per projection thread, at most
+constexpr int kLocSeg = 32;        // expansion orders per thread when filling the table
 
-// Partial projections over one source chunk; Chebyshev polynomials by the three-term
-// recurrence T_{n+1} = 2 x T_n - T_{n-1}.  Thread (l_out, t_out) owns column t0 + t_out and
-// the orders l_out + q LS, q < NL (LS = kLocThreads / BT): NL = 1 for the usual degrees,
-// up to kLocMaxNL for the Wimp degrees of very large orders (hundreds).  `chunk` sources are
-// staged per round so that the KL1 x chunk table fits in shared memory.
+// Partial projections over one source chunk.  The table T_l(x_s) of a chunk is filled in
+// segments of kLocSeg orders, all threads at once: a thread takes one (segment, source)
+// pair, seeds it with cos(m theta) (x = cos theta) for its first two polynomial degrees and
+// steps with T_{m+2} = 2 T_2(x) T_m - T_{m-2} (the degrees of one parity; stable for
+// |x| <= 1), so a Wimp degree in the hundreds costs no long serial recurrence.  Thread
+// (l_out, t_out) owns column t0 + t_out and the orders l_out + q LS, q < NL (LS =
+// kLocThreads / BT): NL = 1 for the usual degrees, up to kLocMaxNL for the degrees of very
+// large orders, which keeps BT (columns per CTA, each CTA refilling the table) large.
+// `chunk` (even) sources are staged per round so that the KL1 x chunk table fits in shared
+// memory.
 template <int NL>
 __global__ void __launch_bounds__(kLocThreads) k_loc_proj(
     const double* __restrict__ rs, const double* __restrict__ cs, int ld_cs, int B,
@@ -41,34 +47,28 @@ __global__ void __launch_bounds__(kLocThreads) k_loc_proj(
   // A box whose sources all sit at r = 0 has r_end = 0; then only the l = 0 term survives
   // (J_l(0) = 0 for l >= 1) and any x works.  The reference divides by zero there.
   const double inv_end = bx.r_end > 0.0 ? 1.0 / bx.r_end : 0.0;
+  const int nseg = (KL1 + kLocSeg - 1) / kLocSeg;
   for (int s0 = 0; s0 < it.nj; s0 += chunk) {
     const int ns = min(chunk, it.nj - s0);
-    for (int s = tid; s < chunk; s += blockDim.x) {
+    for (int e = tid; e < nseg * chunk; e += blockDim.x) {
+      const int sg = e / chunk, s = e - sg * chunk;
+      const int l0 = sg * kLocSeg, l1 = min(KL1, l0 + kLocSeg);
       if (s < ns) {
         double x = rs[it.j0 + s0 + s] * inv_end;
         x = fmin(fmax(x, -1.0), 1.0);
-        double tm1 = 1.0, tc = x;  // T_{n-1}, T_n as n advances
-        int l = 0;
-        for (int nn = 0; l < KL1; ++nn) {
-          double Tn;
-          if (nn == 0) {
-            Tn = 1.0;
-          } else if (nn == 1) {
-            Tn = x;
-          } else {
-            double tn = 2.0 * x * tc - tm1;
-            tm1 = tc;
-            tc = tn;
-            Tn = tn;
-          }
-          int order = odd ? 2 * l + 1 : 2 * l;
-          if (nn == order) {
-            sT[(size_t)l * chunk + s] = odd ? 2.0 * Tn : (l == 0 ? Tn : 2.0 * Tn);
-            ++l;
-          }
+        const double th = acos(x);
+        const int m0 = odd ? 2 * l0 + 1 : 2 * l0;  // degree of order l0
+        double tp = cos((double)(m0 - 2) * th);     // T_{m0-2} (T_{-n} = T_n)
+        double tc = cos((double)m0 * th);           // T_{m0}
+        const double two_t2 = 2.0 * (2.0 * x * x - 1.0);
+        for (int l = l0; l < l1; ++l) {
+          sT[(size_t)l * chunk + s] = (odd || l > 0) ? 2.0 * tc : tc;
+          const double tn = two_t2 * tc - tp;
+          tp = tc;
+          tc = tn;
         }
       } else {
-        for (int l = 0; l < KL1; ++l) sT[(size_t)l * chunk + s] = 0.0;
+        for (int l = l0; l < l1; ++l) sT[(size_t)l * chunk + s] = 0.0;
       }
     }
     for (int e = tid; e < chunk * BT; e += blockDim.x) {
@@ -76,15 +76,27 @@ __global__ void __launch_bounds__(kLocThreads) k_loc_proj(
       sC[s * BT + tt] = (s < ns && t0 + tt < B) ? cs[(size_t)(t0 + tt) * ld_cs + it.j0 + s0 + s] : 0.0;
     }
     __syncthreads();
+    // Sources in pairs: one coefficient load per source serves all NL orders, one 16-byte
+    // table load two multiply-adds (chunk is even, so every pair is 16-byte aligned).
+    const int ns2 = ns & ~1;
+    for (int s = 0; s < ns2; s += 2) {
+      const double c0 = sC[s * BT + t_out], c1 = sC[(s + 1) * BT + t_out];
 #pragma unroll
-    for (int q = 0; q < NL; ++q) {
-      const int l = l_out + q * LS;
-      if (l < KL1) {
-        const double* Tl = sT + (size_t)l * chunk;
-        double a = acc[q];
-#pragma unroll 8
-        for (int s = 0; s < ns; ++s) a = fma(Tl[s], sC[s * BT + t_out], a);
-        acc[q] = a;
+      for (int q = 0; q < NL; ++q) {
+        const int l = l_out + q * LS;
+        if (l < KL1) {
+          const double2 tv = *reinterpret_cast<const double2*>(sT + (size_t)l * chunk + s);
+          acc[q] = fma(tv.x, c0, acc[q]);
+          acc[q] = fma(tv.y, c1, acc[q]);
+        }
+      }
+    }
+    if (ns & 1) {
+      const double c0 = sC[ns2 * BT + t_out];
+#pragma unroll
+      for (int q = 0; q < NL; ++q) {
+        const int l = l_out + q * LS;
+        if (l < KL1) acc[q] = fma(sT[(size_t)l * chunk + ns2], c0, acc[q]);
       }
     }
     __syncthreads();
