@@ -621,7 +621,7 @@ int launch_loc_eval_t(const double* ws, double* gs, int ld_gs, int B, const LocB
                       int neval, const double* d_cheb, int K, int nu_int, double sgn, cudaStream_t st) {
   const int KL1 = K + 1;
   const int BTC = (int)std::max<size_t>(1, std::min<size_t>((size_t)B, kLocSmemDoubles / (size_t)KL1));
-  const size_t sm = sizeof(double) * (size_t)KL1 * BTC;
+  const size_t sm = sizeof(double) * ((size_t)KL1 * BTC + kLocEvalCols);  // rows + register-block padding
   if (sm > 48 * 1024) cudaFuncSetAttribute(k_loc_eval<MAXO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   k_loc_eval<MAXO><<<(unsigned)neval, kLocTargets, sm, st>>>(ws, gs, ld_gs, B, d_box, d_eval, d_cheb, K, nu_int,
                                                             sgn, BTC);

@@ -123,10 +123,14 @@ __global__ void k_loc_reduce(const LocBoxD* __restrict__ boxes, int nbox, int KL
   cheb[e] = s;
 }
 
+constexpr int kLocEvalCols = 16;  // columns accumulated in registers per evaluation pass
+
 // Evaluation at the box's targets: J_0 .. J_maxo at z = k r_end / 2 by Miller's algorithm
 // (local array of MAXO + 1 values per thread), then g[i,t] += sum_l b_l C[l,t] with
 // b_l = J_{l0+odd+l} J_{|l-l0|} (-1)^{max(l-l0,0)}.  The coefficients C of the box are
-// staged in shared memory for BTC columns at a time.
+// staged in shared memory for BTC columns at a time (the rows padded by kLocEvalCols
+// values); each b_l, formed from two reads of the local array, feeds kLocEvalCols columns
+// held in registers, so large Wimp degrees do not re-read the array once per column.
 template <int MAXO>
 __global__ void __launch_bounds__(kLocTargets) k_loc_eval(
     const double* __restrict__ ws, double* __restrict__ gs, int ld_gs, int B,
@@ -161,15 +165,20 @@ __global__ void __launch_bounds__(kLocTargets) k_loc_eval(
     }
     __syncthreads();
     if (!has) continue;
-    for (int tt = 0; tt < nt; ++tt) {
-      double acc = 0.0;
+    for (int tc = 0; tc < nt; tc += kLocEvalCols) {
+      double acc[kLocEvalCols];
+#pragma unroll
+      for (int u = 0; u < kLocEvalCols; ++u) acc[u] = 0.0;
       for (int l = 0; l <= K; ++l) {
         int lo = l > l0 ? l - l0 : l0 - l;
         double v = J[l0 + odd + l] * J[lo];
         if (l > l0 && ((l - l0) & 1)) v = -v;
-        acc = fma(v, s_cheb[l * BTC + tt], acc);
+        const double* row = s_cheb + l * BTC + tc;  // the padding covers row[u] past BTC
+#pragma unroll
+        for (int u = 0; u < kLocEvalCols; ++u) acc[u] = fma(v, row[u], acc[u]);
       }
-      atomicAdd(&gs[(size_t)(tb + tt) * ld_gs + i], sgn * acc);
+      const int nu_c = min(kLocEvalCols, nt - tc);
+      for (int u = 0; u < nu_c; ++u) atomicAdd(&gs[(size_t)(tb + tc + u) * ld_gs + i], sgn * acc[u]);
     }
   }
 }
