@@ -146,12 +146,12 @@ class StdoutToStderr:
         os.close(self.saved)
 
 
-def run_cpu_reference(N, M, B_sample, steps, warmup, threads):
+def run_cpu_reference(N, M, B_sample, runs, threads):
     """The reference's CPU path: oracle/_ref (the reference's own planner and nufht_batch,
     compiled from its sources, over the oracle's evaluators with the type-3 NUFFT), or the
-    oracle's restatement of the driver when oracle/_ref is absent.  Planning (once per
-    direction) is outside the timed region, as the reference's benchmark notebook times
-    nufht_batch.  Returns (seconds per fwd+adj step, kind)."""
+    oracle's restatement of the driver when oracle/_ref is absent, on `threads` host threads.
+    Planning (once per direction) is outside the timed region, as the reference's benchmark
+    notebook times nufht_batch.  Returns (seconds per fwd+adj step of each run, kind)."""
     import oracle
     oracle.set_threads(threads)
     r, k, c, y = make_inputs(N, M, B_sample, 0)
@@ -184,13 +184,37 @@ def run_cpu_reference(N, M, B_sample, steps, warmup, threads):
         def step():
             oracle.nufht_batch(0.0, r, k, cF, 1e-8, mode=oracle.T3_NUFFT)
             oracle.nufht_batch(0.0, k, r, yF, 1e-8, mode=oracle.T3_NUFFT)
-    for _ in range(warmup):
+    times = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
         step()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        step()
-    dt = (time.perf_counter() - t0) / steps
-    return dt, kind
+        times.append(time.perf_counter() - t0)
+    if kind == "reference":
+        for p in plans:
+            R.nufht_plan_free(ctypes.byref(p))
+    return times, kind
+
+
+def cpu_baseline_leg(N, M, B, runs):
+    """CPU baseline of the workload on this box's host: the reference's path on all host
+    threads (OpenMP over columns and the 2(K+1) type-3 transforms of a box; `value`) and on
+    one thread (faithful to the reference, whose only parallel construct is a critical
+    section and whose FINUFFT calls run with nthreads = 1), each the median of `runs` steps
+    of forward + adjoint on a sample of the columns."""
+    cores = os.cpu_count() or 1
+    B_all = max(1, min(B, 8))
+    with StdoutToStderr():
+        t_all, kind = run_cpu_reference(N, M, B_all, runs, cores)
+        t_one, _ = run_cpu_reference(N, M, 1, runs, 1)
+    v_all = 2.0 * (N + M) * B_all / statistics.median(t_all) / 1e9
+    v_one = 2.0 * (N + M) * 1 / statistics.median(t_one) / 1e9
+    return {"value": v_all, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": "%d of %d columns of the workload, fwd+adj, median of %d steps, planning excluded; "
+                      "type-3 transforms by the oracle's NUFFT (eps = tol) in place of FINUFFT" % (B_all, B, runs),
+            "runs_s": t_all,
+            "single_thread": {"value": v_one, "unit": UNIT, "cores": 1, "kind": kind,
+                              "sample": "1 of %d columns, fwd+adj, median of %d steps" % (B, runs),
+                              "runs_s": t_one}}
 
 
 def main():
@@ -218,17 +242,13 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        B_s = max(1, min(B, cores))
-        with StdoutToStderr():
-            dt, kind = run_cpu_reference(N, M, B_s, max(1, min(args.steps, 2)), 0 if args.warmup <= 0 else 1, cores)
-        value = 2.0 * (N + M) * B_s / dt / 1e9
+        cpu = cpu_baseline_leg(N, M, B, 3)
+        value = cpu["value"]
         line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
-                "steps": max(1, min(args.steps, 2)), "warmup": 1, "ms_per_step": dt * 1e3,
+                "steps": 3, "warmup": 0, "ms_per_step": 2.0 * (N + M) * min(B, 8) / value / 1e6,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded numpy draws with the workload's shapes)", "config": config,
-                "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                                 "sample": "%d of %d columns of the workload, fwd+adj, type-3 by the oracle's "
-                                           "NUFFT (eps = tol); planning excluded" % (B_s, B)},
+                "cpu_baseline": cpu,
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -409,29 +429,25 @@ def main():
                             "frac": ach_tf / fp32_peak.value if fp32_peak.value > 0 else None,
                             "peak_source": "measured FP32 packed-FMA probe (nufht_b200_fp32_peak)"}
 
-    # Accuracy of this run's forward output: error against FP64 direct sums (the library's
-    # direct evaluator, every source, no expansion) at 64 sampled targets, per column over
-    # ||c_t||_1, beside the planner's worst-case bound for FP32 rounding (per ||c||_1).
+    # Accuracy of this run's forward output: error against the oracle's exact FP64 direct sums
+    # (every source, no expansion, Kahan-compensated, on the host cores; the checker, outside
+    # every timed region) at 64 sampled targets, per column over ||c_t||_1, beside the
+    # planner's worst-case bound for FP32 rounding (per ||c||_1).
+    import oracle
+    oracle.set_threads(cores)
     pf.execute_columns(c, g, st)
     torch.cuda.synchronize(dev)
     idx = np.sort(np.random.default_rng(7).choice(M, 64, replace=False))
-    ks = np.ascontiguousarray(k[idx])
-    ex = np.zeros((64, B), order="F")
-    cF = np.asfortranarray(c_h.T)
-    lib.add_dir_batch(L.dptr(ex), 0.0, L.dptr(r), L.dptr(cF), L.dptr(ks), N, 64, B, N, 64)
+    ex = oracle.direct_sum(0.0, r, k, c_h.T, idx)
     got = g[:, torch.tensor(idx, device=dev)].cpu().numpy().T
     err = float((np.abs(got - ex).max(axis=0) / np.abs(c_h).sum(axis=1)).max())
     accuracy = {"max_err_over_l1": err, "over_tol": err / tol, "targets_sampled": 64,
-                "reference": "FP64 direct sums (all sources) at sampled targets of the forward transform",
+                "reference": "oracle FP64 direct sums (all sources, host) at sampled targets of the forward transform",
                 "fp32_worst_case_bound_over_l1": float(pf.stats()[14]) if mixed else None}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        B_s = max(1, min(B, cores))
-        with StdoutToStderr():
-            dt, kind = run_cpu_reference(N, M, B_s, 1, 0, cores)
-        cpu = {"value": 2.0 * (N + M) * B_s / dt / 1e9, "unit": UNIT, "cores": cores, "kind": kind,
-               "sample": "%d of %d columns, fwd+adj, planning excluded, type-3 by the oracle's NUFFT" % (B_s, B)}
+        cpu = cpu_baseline_leg(N, M, B, 3)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

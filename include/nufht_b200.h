@@ -250,8 +250,10 @@ int nufht_b200_fp32_peak(double *tflops);
  * forbidden after start-up): adds the local (Wimp) expansion of the single box
  * [0,n) x [0,m) to gs, with its scratch (work lists, partial projections, coefficients) in
  * a 4 MiB device array inside the library that every GPU loading the library holds until
- * exit.  gs, rs, cs, ws are DEVICE pointers; nu is an integer order; asynchronous on
- * `stream`.  Returns 0, -400/-401 (arguments), -2 (order), NUFHT_E_TOO_LARGE when the
+ * exit.  gs, rs, cs, ws are DEVICE pointers of the current device (or managed memory) and
+ * `stream` belongs to it; nu is an integer order (a negative odd order adds the negated
+ * expansion, J_{-n} = (-1)^n J_n); asynchronous on `stream`.  Returns 0, -400/-401
+ * (arguments, including buffers or a stream of another device), -2 (order), NUFHT_E_TOO_LARGE when the
  * scratch would exceed 4 MiB (about ceil(m/2048) (K+1) batch 8 bytes plus work lists),
  * NUFHT_E_CUDA.  The first call on a device looks up the array's address and should come
  * before any stream capture; calls that overlap on the GPU share the array and race. */
@@ -291,6 +293,10 @@ typedef struct {
 
 int nufht_b200_batch_create(NufhtB200Batch **out, const NufhtB200BatchItem *items, int count,
                             int branches);
+/* A batch keeps every plan it uses alive (destroying a plan's handle while a batch uses it
+ * is safe) and pins it: while pinned, running the plan on its own at a larger width gives
+ * it new workspace buffers and leaves the ones the graph recorded allocated until the last
+ * batch using the plan is destroyed.  Items may share a plan at different widths. */
 /* One graph launch on `stream` (a cudaStream_t; asynchronous). */
 int nufht_b200_batch_launch(NufhtB200Batch *batch, void *stream);
 /* Branch count in use, the tuned graph time (ms, 0 when branches was given) and the
@@ -298,6 +304,11 @@ int nufht_b200_batch_launch(NufhtB200Batch *batch, void *stream);
 int nufht_b200_batch_info(const NufhtB200Batch *batch, int *branches, float *tuned_ms,
                           long *kernel_nodes);
 void nufht_b200_batch_destroy(NufhtB200Batch *batch);
+/* Introspection (tests): the plan's current asymptotic-grid workspace, how many older
+ * workspace buffers it keeps allocated for batches that recorded them, and how many
+ * batches pin it. */
+int nufht_b200_plan_buffers(const NufhtDevicePlan *plan, const void **grid, int *retired,
+                            int *pins);
 
 /* Where the planning tables were read from (a cache file path), or "generated". */
 const char *nufht_b200_table_source(void);

@@ -132,6 +132,7 @@ def _declare(lib):
         "nufht_b200_batch_info": (ctypes.c_int, [vp, c_int_p, ctypes.POINTER(ctypes.c_float),
                                                  ctypes.POINTER(ctypes.c_long)]),
         "nufht_b200_batch_destroy": (None, [vp]),
+        "nufht_b200_plan_buffers": (ctypes.c_int, [vp, ctypes.POINTER(vp), c_int_p, c_int_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -6,6 +6,11 @@
 // transform at a time), and the groups are dealt to the branches longest first, each to the
 // branch with the least estimated work so far.  With branches = 0 the branch count is tuned
 // at creation by timing the graph for 1, 2, 4, ... 32 branches on the items' own buffers.
+//
+// The graph records each plan's workspace pointers and cuFFT plans.  So the batch holds a
+// reference to every plan (a plan outlives its handle while a batch uses it) and pins it:
+// while pinned, a standalone run that needs a larger workspace gets new buffers and the old
+// ones stay allocated for the graph; cuFFT plans are kept per batch width and never remade.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,6 +30,8 @@ using hankel::DevicePlan;
 struct NufhtB200Batch {
   int device = 0;
   std::vector<NufhtB200BatchItem> items;
+  std::vector<std::shared_ptr<DevicePlan>> item_plan;  // plan of each item
+  std::vector<std::shared_ptr<DevicePlan>> plans;      // distinct plans of the items, pinned
   int branches = 0;
   long kernel_nodes = 0;
   float tuned_ms = 0.0f;
@@ -42,6 +49,10 @@ struct NufhtB200Batch {
   }
   ~NufhtB200Batch() {
     release_graph();
+    for (auto& D : plans) {
+      std::lock_guard<std::mutex> lk(D->mu);
+      D->unpin();
+    }
     for (cudaStream_t s : streams) cudaStreamDestroy(s);
     for (cudaEvent_t e : joins) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
@@ -51,9 +62,9 @@ struct NufhtB200Batch {
 namespace {
 
 // Estimated device work of one item (multiply-adds; Bessel evaluations weighted as ~16).
-double item_cost(const NufhtB200BatchItem& it) {
+double item_cost(const DevicePlan& D, const NufhtB200BatchItem& it) {
   double st[12];
-  hankel::plan_stats(*it.plan->dp, st, 12);
+  hankel::plan_stats(D, st, 12);
   const double B = it.batch;
   return B * st[10] * (st[3] + st[4]) + B * st[10] * st[9] / 4.0 + (16.0 + B) * st[5] +
          B * st[11] * (st[6] + st[7]);
@@ -82,9 +93,9 @@ int capture(NufhtB200Batch* b, int nb) {
   std::map<DevicePlan*, std::vector<int>> groups;
   std::map<DevicePlan*, double> gcost;
   for (int i = 0; i < (int)b->items.size(); ++i) {
-    DevicePlan* D = b->items[i].plan->dp.get();
+    DevicePlan* D = b->item_plan[i].get();
     groups[D].push_back(i);
-    gcost[D] += item_cost(b->items[i]);
+    gcost[D] += item_cost(*D, b->items[i]);
   }
   std::vector<DevicePlan*> order;
   for (auto& kv : groups) order.push_back(kv.first);
@@ -109,7 +120,7 @@ int capture(NufhtB200Batch* b, int nb) {
   for (int br = 0; br < nb && !rc; ++br) {
     for (int i : lanes[br]) {
       const NufhtB200BatchItem& it = b->items[i];
-      DevicePlan* D = it.plan->dp.get();
+      DevicePlan* D = b->item_plan[i].get();
       std::lock_guard<std::mutex> lk(D->mu);
       rc = D->run(it.cs, it.ld_cs, it.gs, it.ld_gs, it.batch, b->streams[br], true);
       if (rc) break;
@@ -190,17 +201,31 @@ int nufht_b200_batch_create(NufhtB200Batch** out, const NufhtB200BatchItem* item
   std::unique_ptr<NufhtB200Batch> b(new NufhtB200Batch);
   b->device = device;
   b->items.assign(items, items + count);
+  for (const NufhtB200BatchItem& it : b->items) b->item_plan.push_back(it.plan->dp);
   if (cudaSetDevice(device) != cudaSuccess) return NUFHT_E_CUDA;
   int rc = ensure_streams(b.get(), 1);
   if (rc) return rc;
-  // One ordinary pass first: sizes every workspace and FFT plan for its batch width and sets
-  // kernel attributes, so that nothing allocates while the graph is captured.
-  for (const NufhtB200BatchItem& it : b->items) {
-    DevicePlan* D = it.plan->dp.get();
+  // One ordinary pass first, widest items first: sizes every workspace for its plan's widest
+  // item, makes the FFT plans of every width and sets kernel attributes, so that nothing
+  // allocates while the graph is captured (items that share a plan may differ in width).
+  std::vector<int> warm(count);
+  std::iota(warm.begin(), warm.end(), 0);
+  std::stable_sort(warm.begin(), warm.end(),
+                   [&](int a, int c) { return b->items[a].batch > b->items[c].batch; });
+  for (int i : warm) {
+    const NufhtB200BatchItem& it = b->items[i];
+    DevicePlan* D = b->item_plan[i].get();
     std::lock_guard<std::mutex> lk(D->mu);
     if ((rc = D->run(it.cs, it.ld_cs, it.gs, it.ld_gs, it.batch, b->streams[0], true))) return rc;
   }
   if (cudaStreamSynchronize(b->streams[0]) != cudaSuccess) return NUFHT_E_CUDA;
+  // Pin the plans before the first capture (the destructor unpins them).
+  for (const std::shared_ptr<DevicePlan>& D : b->item_plan) {
+    if (std::find(b->plans.begin(), b->plans.end(), D) != b->plans.end()) continue;
+    std::lock_guard<std::mutex> lk(D->mu);
+    D->pin();
+    b->plans.push_back(D);
+  }
   if (branches > 0) {
     if ((rc = capture(b.get(), std::min(branches, count)))) return rc;
   } else {
@@ -242,6 +267,16 @@ void nufht_b200_batch_destroy(NufhtB200Batch* b) {
   if (!b) return;
   cudaSetDevice(b->device);
   delete b;
+}
+
+int nufht_b200_plan_buffers(const NufhtDevicePlan* plan, const void** grid, int* retired, int* pins) {
+  if (!plan) return -400;
+  DevicePlan* D = plan->dp.get();
+  std::lock_guard<std::mutex> lk(D->mu);
+  if (grid) *grid = D->d_grid;
+  if (retired) *retired = (int)D->retired.size();
+  if (pins) *pins = D->pins;
+  return 0;
 }
 
 }  // extern "C"

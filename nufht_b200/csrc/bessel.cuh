@@ -29,7 +29,7 @@ __device__ __forceinline__ int miller_start(int M) {
   return (N + 1) & ~1;
 }
 
-// J_0(x) and J_1(x) for x >= 25 from Hankel's expansion (Abramowitz & Stegun 9.2.5-9.2.10)
+// J_0(x) and J_1(x) for x >= 17 from Hankel's expansion (Abramowitz & Stegun 9.2.5-9.2.10)
 //   J_nu(x) = sqrt(2/(pi x)) (P_nu cos chi - Q_nu sin chi),  chi = x - (nu/2 + 1/4) pi,
 //   P_nu = sum_k (-1)^k a_2k(nu) / x^2k,  Q_nu = sum_k (-1)^k a_2k+1(nu) / x^2k+1,
 //   a_0 = 1,  a_k = a_{k-1} (4 nu^2 - (2k-1)^2) / (8k),

@@ -6,6 +6,8 @@
 
 #include "executor.h"
 
+// Shared ownership: a batch (batch.cpp) keeps the plans it captured alive after the caller
+// destroys the handle.
 struct NufhtDevicePlan {
-  std::unique_ptr<hankel::DevicePlan> dp;
+  std::shared_ptr<hankel::DevicePlan> dp;
 };

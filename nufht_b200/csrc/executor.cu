@@ -505,12 +505,31 @@ int DevicePlan::upload_all() {
 }
 
 void DevicePlan::release_fft() {
-  for (FftGroup& g : groups)
-    if (g.plan) {
-      cufftDestroy(g.plan);
-      g.plan = 0;
-    }
+  for (auto& kv : fft_cache)
+    for (cufftHandle h : kv.second) cufftDestroy(h);
+  fft_cache.clear();
+  for (FftGroup& g : groups) g.plan = 0;
   fft_B = 0;
+}
+
+void DevicePlan::drop_buffer(void* p) {
+  if (!p) return;
+  if (pins > 0) retired.push_back(p);
+  else cudaFree(p);
+}
+
+void DevicePlan::pin() { ++pins; }
+
+void DevicePlan::unpin() {
+  if (pins > 0) --pins;
+  if (pins > 0 || retired.empty()) return;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  cudaDeviceSynchronize();  // a launch of a released graph may still read them
+  for (void* p : retired) cudaFree(p);
+  retired.clear();
+  if (prev >= 0) cudaSetDevice(prev);
 }
 
 DevicePlan::~DevicePlan() {
@@ -522,6 +541,7 @@ DevicePlan::~DevicePlan() {
   cudaFree(d_dir); cudaFree(d_asyb); cudaFree(d_spread); cudaFree(d_interp);
   cudaFree(d_corr); cudaFree(d_post);
   cudaFree(d_grid); cudaFree(d_partial); cudaFree(d_cheb); cudaFree(d_fft_work);
+  for (void* p : retired) cudaFree(p);
   cudaFree(d_stage_c); cudaFree(d_stage_g); cudaFree(d_stage_t);
   if (copy_in) cudaStreamDestroy(copy_in);
   if (copy_out) cudaStreamDestroy(copy_out);
@@ -533,47 +553,65 @@ DevicePlan::~DevicePlan() {
 }
 
 // FFT plans for batch size B: group g transforms nbox * V contiguous vectors of length n2.
-// Plans are remade when B changes.
+// Plans are made once per batch size and kept (a captured batch graph may refer to the plans
+// of any size it used); the shared work area only grows.
 int DevicePlan::ensure_fft(int B) {
   if (asyb.empty() || B == fft_B) return 0;
-  release_fft();
-  const long long V = (long long)NLP * B;
-  size_t need = 0;
-  for (FftGroup& gr : groups) {
-    cufftHandle h;
-    if (cufftCreate(&h) != CUFFT_SUCCESS) return NUFHT_E_CUDA;
-    cufftSetAutoAllocation(h, 0);
-    int nn = gr.n2;
-    long long batch = (long long)gr.nbox * V;
-    if (batch > INT_MAX) {
-      cufftDestroy(h);
-      return NUFHT_E_TOO_LARGE;
+  auto it = fft_cache.find(B);
+  if (it == fft_cache.end()) {
+    const long long V = (long long)NLP * B;
+    size_t need = 0;
+    std::vector<cufftHandle> hs;
+    auto destroy = [&]() {
+      for (cufftHandle h : hs) cufftDestroy(h);
+    };
+    for (FftGroup& gr : groups) {
+      cufftHandle h;
+      if (cufftCreate(&h) != CUFFT_SUCCESS) {
+        destroy();
+        return NUFHT_E_CUDA;
+      }
+      hs.push_back(h);
+      cufftSetAutoAllocation(h, 0);
+      int nn = gr.n2;
+      long long batch = (long long)gr.nbox * V;
+      if (batch > INT_MAX) {
+        destroy();
+        return NUFHT_E_TOO_LARGE;
+      }
+      size_t wsz = 0;
+      if (cufftMakePlanMany(h, 1, &nn, nullptr, 1, nn, nullptr, 1, nn, mixed_asy ? CUFFT_C2C : CUFFT_Z2Z,
+                            (int)batch, &wsz) != CUFFT_SUCCESS) {
+        destroy();
+        std::fprintf(stderr, "nufht_b200: cufftMakePlanMany failed (n=%d batch=%lld)\n", nn, batch);
+        return NUFHT_E_CUDA;
+      }
+      need = std::max(need, wsz);
     }
-    size_t wsz = 0;
-    if (cufftMakePlanMany(h, 1, &nn, nullptr, 1, nn, nullptr, 1, nn, mixed_asy ? CUFFT_C2C : CUFFT_Z2Z, (int)batch, &wsz) !=
-        CUFFT_SUCCESS) {
-      cufftDestroy(h);
-      std::fprintf(stderr, "nufht_b200: cufftMakePlanMany failed (n=%d batch=%lld)\n", nn, batch);
-      return NUFHT_E_CUDA;
+    if (need > fft_work_bytes) {
+      drop_buffer(d_fft_work);
+      d_fft_work = nullptr;
+      fft_work_bytes = 0;
+      if (cudaMalloc(&d_fft_work, need) != cudaSuccess) {
+        destroy();
+        std::fprintf(stderr, "nufht_b200: cudaMalloc of %zu bytes of FFT work area failed\n", need);
+        return NUFHT_E_CUDA;
+      }
+      fft_work_bytes = need;
+      for (auto& kv : fft_cache)
+        for (cufftHandle h : kv.second) cufftSetWorkArea(h, d_fft_work);
     }
-    need = std::max(need, wsz);
-    gr.plan = h;
+    for (cufftHandle h : hs) cufftSetWorkArea(h, d_fft_work);
+    it = fft_cache.emplace(B, std::move(hs)).first;
   }
-  if (need > fft_work_bytes) {
-    cudaFree(d_fft_work);
-    d_fft_work = nullptr;
-    fft_work_bytes = 0;
-    NUFHT_CUDA_TRY(cudaMalloc(&d_fft_work, need));
-    fft_work_bytes = need;
-  }
-  for (FftGroup& gr : groups) cufftSetWorkArea(gr.plan, d_fft_work);
+  for (size_t g = 0; g < groups.size(); ++g) groups[g].plan = it->second[g];
   fft_B = B;
   return 0;
 }
 
 int DevicePlan::ensure_workspace(int B) {
   if (B <= ws_B) return ensure_fft(B);
-  cudaFree(d_grid); cudaFree(d_partial); cudaFree(d_cheb);
+  drop_buffer(d_grid); drop_buffer(d_partial); drop_buffer(d_cheb);
   d_grid = nullptr; d_partial = nullptr; d_cheb = nullptr;
   ws_B = 0;
   size_t bytes = 0;
@@ -718,9 +756,9 @@ int DevicePlan::run(const double* cs, int ld_cs, double* gs, int ld_gs, int B, c
 // contribution.  Used by the allocation-free entry point (noalloc.cu).
 int run_loc_box(const double* rs, const double* ws, const double* cs, int ld_cs, double* gs, int ld_gs,
                 int B, const LocBoxD* d_box, const ProjItem* d_proj, int nproj, const EvalItem* d_eval,
-                int neval, double* d_partial, double* d_cheb, int K, int nu_int, cudaStream_t st) {
+                int neval, double* d_partial, double* d_cheb, int K, int nu_int, double sgn, cudaStream_t st) {
   return launch_loc(rs, ws, cs, ld_cs, gs, ld_gs, B, d_box, 1, d_proj, nproj, d_eval, neval, d_partial, d_cheb, K,
-                    nu_int, 1.0, st);
+                    nu_int, sgn, st);
 }
 
 int run_besselj(double nu, const double* x, double* out, long count, cudaStream_t st) {

@@ -5,6 +5,7 @@
 #include <cufft.h>
 
 #include <atomic>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -125,8 +126,14 @@ struct DevicePlan {
 
   // workspace, sized for the largest batch executed so far
   int ws_B = 0;
-  int fft_B = 0;             // batch size the FFT plans were made for
+  int fft_B = 0;             // batch size of the FFT plans in groups[].plan
+  std::map<int, std::vector<cufftHandle>> fft_cache;  // FFT plans per batch size, one per group
   size_t fft_work_bytes = 0;
+  // Batches (CUDA graphs) that recorded this plan's buffers and FFT plans: while pins > 0 a
+  // buffer that must grow is replaced by a new allocation and the old one is kept in
+  // `retired` (the graphs still use it) until the last batch lets go.
+  int pins = 0;
+  std::vector<void*> retired;
   size_t ws_bytes = 0;
   void* d_grid = nullptr;    // complex FP64 (double2) or, in mixed precision, FP32 (float2)
   bool mixed_asy = false;    // asymptotic boxes in FP32 (NUFHT_B200_MIXED, where FP32 meets tol)
@@ -153,6 +160,9 @@ struct DevicePlan {
   int ensure_workspace(int B);
   int ensure_fft(int B);
   void release_fft();
+  void drop_buffer(void* p);  // cudaFree, or keep in `retired` while pinned
+  void pin();                 // called with mu held
+  void unpin();               // called with mu held; frees retired buffers at zero pins
   // g (+)= H c on stream st; cs / gs are device pointers.
   int run(const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
           bool zero_output);
@@ -213,5 +223,5 @@ int fp64_peak(double* tflops);
 namespace hankel {
 int run_loc_box(const double* rs, const double* ws, const double* cs, int ld_cs, double* gs, int ld_gs,
                 int B, const LocBoxD* d_box, const ProjItem* d_proj, int nproj, const EvalItem* d_eval,
-                int neval, double* d_partial, double* d_cheb, int K, int nu_int, cudaStream_t st);
+                int neval, double* d_partial, double* d_cheb, int K, int nu_int, double sgn, cudaStream_t st);
 }  // namespace hankel

@@ -89,13 +89,15 @@ __global__ void k_noalloc_loc_items(const double* __restrict__ rs, int m, int n,
   }
 }
 
-bool on_device(const void* p) {
+// Device memory of the current device (or managed memory, which any device can reach).
+bool on_current_device(const void* p, int dev) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 }  // namespace
@@ -108,8 +110,24 @@ extern "C" int nufht_b200_add_loc_batch_noalloc(double* gs, double nu, const dou
   if (!gs || !rs || !cs || !ws || m <= 0 || n <= 0 || batch <= 0 || K < 0) return -400;
   if (ld_cs < m || ld_gs < n) return -401;
   if (!is_integer(nu) || std::fabs(nu) > 200.0) return -2;
-  if (!on_device(gs) || !on_device(rs) || !on_device(cs) || !on_device(ws)) return -400;
+  // Every buffer, and the stream, must belong to the current device: the kernels and the
+  // scratch array used are the current device's.
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return NUFHT_E_CUDA;
+  if (!on_current_device(gs, dev) || !on_current_device(rs, dev) || !on_current_device(cs, dev) ||
+      !on_current_device(ws, dev))
+    return -400;
+  if (stream) {
+    int sdev = -1;
+    if (cudaStreamGetDevice((cudaStream_t)stream, &sdev) != cudaSuccess) {
+      cudaGetLastError();
+      return -400;
+    }
+    if (sdev != dev) return -400;
+  }
   const int nu_int = (int)std::llround(std::fabs(nu));
+  // J_{-n} = (-1)^n J_n: odd negative orders add the negated expansion.
+  const double sgn = (nu < 0.0 && (nu_int & 1)) ? -1.0 : 1.0;
   const int KL1 = K + 1;
   if (KL1 > 256 || nu_int / 2 + K + (nu_int & 1) > 512) return NUFHT_E_TOO_LARGE;
   const int nproj = (m + kNoAllocLocSources - 1) / kNoAllocLocSources;
@@ -136,5 +154,5 @@ extern "C" int nufht_b200_add_loc_batch_noalloc(double* gs, double nu, const dou
   g_launch_counter.fetch_add(1, std::memory_order_relaxed);
   if (cudaGetLastError() != cudaSuccess) return NUFHT_E_CUDA;
   return run_loc_box(rs, ws, cs, ld_cs, gs, ld_gs, batch, d_box, d_proj, nproj, d_eval, neval, d_part, d_cheb, K,
-                     nu_int, st);
+                     nu_int, sgn, st);
 }

@@ -67,6 +67,15 @@ class DevicePlan:
         L.lib().nufht_b200_plan_info(self._h, ctypes.byref(inf))
         return {f: getattr(inf, f) for f, _ in inf._fields_}
 
+    def buffers(self):
+        """(current asymptotic-grid workspace address, older workspace buffers kept for batch
+        graphs that recorded them, number of batches pinning the plan)."""
+        g = ctypes.c_void_p()
+        ret = ctypes.c_int()
+        pins = ctypes.c_int()
+        L.lib().nufht_b200_plan_buffers(self._h, ctypes.byref(g), ctypes.byref(ret), ctypes.byref(pins))
+        return g.value, ret.value, pins.value
+
     def boxes(self):
         lib = L.lib()
         tot = lib.nufht_b200_plan_boxes(self._h, None, 0)

@@ -397,80 +397,119 @@ static double o_ker_hat(const OKer *K, double om) /* int psi(u) cos(om u) du */
     return 2.0 * s;
 }
 
-static int o_type3_nufft(int ntr, int nj, const double *xj, const double *cj, double eps,
-                         int nk, const double *sk, double *fk)
+/* Per-box setup of the type-3 transform: grid geometry, kernel weights and phases of the
+ * sources and targets, deconvolution factors.  The reference calls finufft1d3many 2(K+1)
+ * times per box on the same points (src/expansions.c:499-557); the stand-in keeps the last
+ * setup of each thread and reuses it when the next call has the same points, which makes
+ * the CPU baseline faster than per-call setup, never slower. */
+typedef struct {
+    const double *xj, *sk;
+    int nj, nk;
+    double eps;
+    int w;
+    double C, D, h;
+    long half, n2;
+    double *wts, *ph, *corr, *kw, *post;
+    long *l0s, *q0s;
+} O3Setup;
+
+static __thread O3Setup t3_cache;
+
+static void o3_free(O3Setup *S)
 {
+    free(S->wts); free(S->ph); free(S->corr); free(S->kw); free(S->post); free(S->l0s); free(S->q0s);
+    memset(S, 0, sizeof(*S));
+}
+
+static int o3_setup(O3Setup *S, int nj, const double *xj, double eps, int nk, const double *sk)
+{
+    if (S->wts && S->xj == xj && S->nj == nj && S->sk == sk && S->nk == nk && S->eps == eps) return 0;
+    o3_free(S);
     OKer K; o_ker_init(&K, eps);
     int w = K.w;
     double xmin = xj[0], xmax = xj[0], smin = sk[0], smax = sk[0];
     for (int j = 1; j < nj; ++j) { if (xj[j] < xmin) xmin = xj[j]; if (xj[j] > xmax) xmax = xj[j]; }
     for (int k = 1; k < nk; ++k) { if (sk[k] < smin) smin = sk[k]; if (sk[k] > smax) smax = sk[k]; }
     double C = 0.5 * (xmin + xmax), X = 0.5 * (xmax - xmin);
-    double D = 0.5 * (smin + smax), S = 0.5 * (smax - smin);
-    if (S < 1e-12 * (fabs(D) + 1.0)) S = 1e-12 * (fabs(D) + 1.0);
-    double h = M_PI / (2.0 * S);
+    double D = 0.5 * (smin + smax), S_ = 0.5 * (smax - smin);
+    if (S_ < 1e-12 * (fabs(D) + 1.0)) S_ = 1e-12 * (fabs(D) + 1.0);
+    double h = M_PI / (2.0 * S_);
     long half = (long)ceil(X / h + 0.5 * w);
     long L1 = 2 * half + 1;
     long n2 = 2;
     while (n2 < 2 * L1) n2 *= 2;
     if (n2 > (1L << 28)) return -1;
-    double *b = (double *)malloc(sizeof(double) * 2 * (size_t)n2);
-    double *wts = (double *)malloc(sizeof(double) * (size_t)w * (size_t)nj);
-    long *l0s = (long *)malloc(sizeof(long) * (size_t)nj);
-    double *ph = (double *)malloc(sizeof(double) * 2 * (size_t)nj);
-    double *corr = (double *)malloc(sizeof(double) * (size_t)L1);
-    double *kw = (double *)malloc(sizeof(double) * (size_t)w * (size_t)nk);
-    long *q0s = (long *)malloc(sizeof(long) * (size_t)nk);
-    double *post = (double *)malloc(sizeof(double) * 2 * (size_t)nk);
-    if (!b || !wts || !l0s || !ph || !corr || !kw || !q0s || !post) return -2;
+    S->wts = (double *)malloc(sizeof(double) * (size_t)w * (size_t)nj);
+    S->l0s = (long *)malloc(sizeof(long) * (size_t)nj);
+    S->ph = (double *)malloc(sizeof(double) * 2 * (size_t)nj);
+    S->corr = (double *)malloc(sizeof(double) * (size_t)L1);
+    S->kw = (double *)malloc(sizeof(double) * (size_t)w * (size_t)nk);
+    S->q0s = (long *)malloc(sizeof(long) * (size_t)nk);
+    S->post = (double *)malloc(sizeof(double) * 2 * (size_t)nk);
+    if (!S->wts || !S->l0s || !S->ph || !S->corr || !S->kw || !S->q0s || !S->post) { o3_free(S); return -2; }
     for (int j = 0; j < nj; ++j) {
         double x = xj[j] - C, u = x / h;
         long l0 = (long)ceil(u - 0.5 * w);
-        l0s[j] = l0;
-        for (int t = 0; t < w; ++t) wts[(size_t)j * w + t] = o_es((double)(l0 + t) - u, w, K.beta);
-        ph[2 * j] = cos(D * x); ph[2 * j + 1] = sin(D * x);
+        S->l0s[j] = l0;
+        for (int t = 0; t < w; ++t) S->wts[(size_t)j * w + t] = o_es((double)(l0 + t) - u, w, K.beta);
+        S->ph[2 * j] = cos(D * x); S->ph[2 * j + 1] = sin(D * x);
     }
-    for (long l = -half; l <= half; ++l) corr[l + half] = 1.0 / o_ker_hat(&K, 2.0 * M_PI * l / n2);
+    for (long l = -half; l <= half; ++l) S->corr[l + half] = 1.0 / o_ker_hat(&K, 2.0 * M_PI * l / n2);
     for (int k = 0; k < nk; ++k) {
         double th = (sk[k] - D) * h, u = th * n2 / (2.0 * M_PI);
         long q0 = (long)ceil(u - 0.5 * w);
-        q0s[k] = q0;
-        for (int t = 0; t < w; ++t) kw[(size_t)k * w + t] = o_es(u - (double)(q0 + t), w, K.beta);
+        S->q0s[k] = q0;
+        for (int t = 0; t < w; ++t) S->kw[(size_t)k * w + t] = o_es(u - (double)(q0 + t), w, K.beta);
         double sc = 1.0 / o_ker_hat(&K, th);
-        post[2 * k] = sc * cos(sk[k] * C); post[2 * k + 1] = sc * sin(sk[k] * C);
+        S->post[2 * k] = sc * cos(sk[k] * C); S->post[2 * k + 1] = sc * sin(sk[k] * C);
     }
+    S->xj = xj; S->sk = sk; S->nj = nj; S->nk = nk; S->eps = eps;
+    S->w = w; S->C = C; S->D = D; S->h = h; S->half = half; S->n2 = n2;
+    return 0;
+}
+
+static int o_type3_nufft(int ntr, int nj, const double *xj, const double *cj, double eps,
+                         int nk, const double *sk, double *fk)
+{
+    O3Setup *S = &t3_cache;
+    int rc = o3_setup(S, nj, xj, eps, nk, sk);
+    if (rc) return rc;
+    const int w = S->w;
+    const long half = S->half, n2 = S->n2;
+    double *b = (double *)malloc(sizeof(double) * 2 * (size_t)n2);
+    if (!b) return -2;
     for (int tr = 0; tr < ntr; ++tr) {
         const double *c = cj + 2 * (size_t)tr * nj;
         double *f = fk + 2 * (size_t)tr * nk;
         memset(b, 0, sizeof(double) * 2 * (size_t)n2);
         for (int j = 0; j < nj; ++j) {
-            double ar = c[2 * j] * ph[2 * j] - c[2 * j + 1] * ph[2 * j + 1];
-            double ai = c[2 * j] * ph[2 * j + 1] + c[2 * j + 1] * ph[2 * j];
+            double ar = c[2 * j] * S->ph[2 * j] - c[2 * j + 1] * S->ph[2 * j + 1];
+            double ai = c[2 * j] * S->ph[2 * j + 1] + c[2 * j + 1] * S->ph[2 * j];
             for (int t = 0; t < w; ++t) {
-                long l = l0s[j] + t;
+                long l = S->l0s[j] + t;
                 long idx = ((l % n2) + n2) % n2;
-                double wv = wts[(size_t)j * w + t];
+                double wv = S->wts[(size_t)j * w + t];
                 b[2 * idx] += wv * ar; b[2 * idx + 1] += wv * ai;
             }
         }
         for (long l = -half; l <= half; ++l) {
             long idx = ((l % n2) + n2) % n2;
-            b[2 * idx] *= corr[l + half]; b[2 * idx + 1] *= corr[l + half];
+            b[2 * idx] *= S->corr[l + half]; b[2 * idx + 1] *= S->corr[l + half];
         }
         o_fft_pos(b, (int)n2);
         for (int k = 0; k < nk; ++k) {
             double sr = 0.0, si = 0.0;
             for (int t = 0; t < w; ++t) {
-                long q = q0s[k] + t;
+                long q = S->q0s[k] + t;
                 long idx = ((q % n2) + n2) % n2;
-                double wv = kw[(size_t)k * w + t];
+                double wv = S->kw[(size_t)k * w + t];
                 sr += wv * b[2 * idx]; si += wv * b[2 * idx + 1];
             }
-            f[2 * k] = sr * post[2 * k] - si * post[2 * k + 1];
-            f[2 * k + 1] = sr * post[2 * k + 1] + si * post[2 * k];
+            f[2 * k] = sr * S->post[2 * k] - si * S->post[2 * k + 1];
+            f[2 * k + 1] = sr * S->post[2 * k + 1] + si * S->post[2 * k];
         }
     }
-    free(b); free(wts); free(l0s); free(ph); free(corr); free(kw); free(q0s); free(post);
+    free(b);
     return 0;
 }
 

@@ -7,7 +7,7 @@
   e2e_golden.npz     outputs of the reference's own nufht_plan_init + nufht_batch control
                      flow (oracle/_ref) over the oracle's evaluators with exact type-3 sums
 
-Usage: python tests/golden/make_golden.py   (needs the reference tree and mpmath)
+Usage: NUFHT_REFERENCE_DIR=<reference tree> python tests/golden/make_golden.py   (needs mpmath)
 """
 import math
 import os
@@ -18,7 +18,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-REF_DIR = os.environ.get("NUFHT_REFERENCE_DIR", "/root/reference")
+REF_DIR = os.environ.get("NUFHT_REFERENCE_DIR")
+if __name__ == "__main__" and not REF_DIR:
+    sys.exit("make_golden.py: set NUFHT_REFERENCE_DIR to the reference tree (it reads the table "
+             "cache and builds the reference's planner from it)")
 
 
 def grids(kind, m, n, seed):

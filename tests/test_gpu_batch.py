@@ -80,3 +80,46 @@ def test_graph_batch_fixed_branches_and_relaunch(cuda):
     for a, b in zip(first, second):
         assert torch.allclose(b, 2.0 * a, rtol=0, atol=1e-12 * float(a.abs().max()) + 1e-300)
     tb.close()
+
+
+def test_graph_batch_shared_plan_widths_and_pinning(cuda):
+    """Items that share a plan at different widths, and a standalone run of a batched plan at a
+    larger width: the batch keeps the buffers its graph recorded (pinned plan), so later
+    launches still give the plan's results; destroying the batch releases the old buffers.
+    The plan's handle may also be closed while the batch still uses it."""
+    import torch
+    from nufht_b200 import DevicePlan
+    from nufht_b200.batch import TransformBatch
+    rng = np.random.default_rng(6)
+    r = np.sort(300.0 * (1.0 - rng.random(20000)))
+    k = np.sort(200.0 * (1.0 - rng.random(15000)))
+    p = DevicePlan(0.0, r, k, 1e-8)
+    q = DevicePlan(1.0, k, r, 1e-8)
+    ca = torch.tensor(rng.standard_normal((3, 20000)), device=cuda)
+    cb = torch.tensor(rng.standard_normal((7, 20000)), device=cuda)
+    cq = torch.tensor(rng.standard_normal((5, 15000)), device=cuda)
+    ref = [p.execute_columns(ca).clone(), p.execute_columns(cb).clone(), q.execute_columns(cq).clone()]
+    tb = TransformBatch([(p, ca), (p, cb), (q, cq)], branches=2)
+    grid0, retired0, pins = p.buffers()
+    assert pins == 1 and retired0 == 0
+    out = [o.clone() for o in tb.launch()]
+    torch.cuda.synchronize()
+    for a, b in zip(out, ref):
+        assert torch.allclose(a, b, rtol=0, atol=1e-12 * float(b.abs().max()))
+    # the plan alone at a larger width: new workspace, the graph's one kept
+    wide = torch.tensor(rng.standard_normal((24, 20000)), device=cuda)
+    wide_out = p.execute_columns(wide).clone()
+    grid1, retired1, _ = p.buffers()
+    assert grid1 != grid0 and retired1 >= 1
+    q.close()  # the batch still holds the plan
+    for o in tb.outputs:
+        o.fill_(np.nan)
+    out2 = tb.launch()
+    torch.cuda.synchronize()
+    for a, b in zip(out2, ref):
+        assert torch.allclose(a, b, rtol=0, atol=1e-12 * float(b.abs().max()))
+    tb.close()
+    _, retired2, pins2 = p.buffers()
+    assert pins2 == 0 and retired2 == 0
+    assert torch.allclose(p.execute_columns(wide), wide_out, rtol=0, atol=1e-12 * float(wide_out.abs().max()))
+    p.close()

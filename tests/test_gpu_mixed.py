@@ -154,24 +154,36 @@ def test_reference_entry_point_precision_switch(cuda, orc):
         assert col_err(g, orc.nufht_batch(0.0, r, k, c, tol), c).max() <= tol
 
 
-@pytest.mark.parametrize("tol", [1e-6, 1e-10])
-def test_cfg2_full_size_tolerances(cuda, orc, tol):
-    """N = M = 1e6 on (0, 1000], batch 32 of N(0,1), tol 1e-6 and 1e-10: the plain FP64 form
-    and both mixed forms against FP64 direct sums (every source, no expansion; the library's
-    direct evaluator) at 2000 sampled targets."""
-    import torch
-    from nufht_b200 import DevicePlan
-    from nufht_b200 import _lib as L
+@pytest.fixture(scope="module")
+def cfg2_exact(orc):
+    """The 1e6-point workload (N = M = 1e6 on (0, 1000], batch 32 of N(0,1)) and the oracle's
+    exact FP64 direct sums (every source, Kahan-compensated, on all host cores) at 2000
+    sampled targets."""
     N, B = 1_000_000, 32
     rng = np.random.default_rng(1)
     r = np.sort(1000.0 * (1.0 - rng.random(N)))
     k = np.sort(1000.0 * (1.0 - rng.random(N)))
     c = np.random.default_rng(2).standard_normal((N, B))
     idx = np.sort(np.random.default_rng(3).choice(N, 2000, replace=False))
+    ex = orc.direct_sum(0.0, r, k, c, idx)
+    return r, k, c, idx, ex
+
+
+@pytest.mark.parametrize("tol", [1e-6, 1e-8, 1e-10])
+def test_cfg2_full_size_tolerances(cuda, cfg2_exact, tol):
+    """N = M = 1e6 on (0, 1000], batch 32 of N(0,1), tol 1e-6, 1e-8 and 1e-10: the plain FP64
+    form and both mixed forms against the oracle's FP64 direct sums at 2000 sampled targets
+    (32 columns), and the library's own GPU direct evaluator as a second cross-check."""
+    import torch
+    from nufht_b200 import DevicePlan
+    from nufht_b200 import _lib as L
+    r, k, c, idx, ex = cfg2_exact
+    N, B = c.shape
     ks = np.ascontiguousarray(k[idx])
-    ex = np.zeros((2000, B), order="F")
+    gd = np.zeros((len(idx), B), order="F")
     cf = np.asfortranarray(c)
-    L.lib().add_dir_batch(L.dptr(ex), 0.0, L.dptr(r), L.dptr(cf), L.dptr(ks), N, 2000, B, N, 2000)
+    L.lib().add_dir_batch(L.dptr(gd), 0.0, L.dptr(r), L.dptr(cf), L.dptr(ks), N, len(idx), B, N, len(idx))
+    assert col_err(gd, ex, c).max() <= 1e-12
     ct = torch.tensor(c, device=cuda)
     it = torch.tensor(idx, device=cuda)
     for mixed in (False, True, "averaged"):

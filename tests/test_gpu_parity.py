@@ -288,6 +288,30 @@ def test_single_box_evaluators(cuda, orc, kind):
     assert col_err(g - g0, gd, c).max() <= 1e-8
 
 
+@pytest.mark.parametrize("nu", [0.0, 1.0, 10.0, 100.0])
+@pytest.mark.parametrize("shape", ["thin", "tall"])
+def test_direct_box_large_against_oracle(cuda, orc, nu, shape):
+    """add_dir_batch (the direct-box kernel) on large boxes whose k r runs through the
+    transition region of J_nu (0 < k r <= 300): thin (48 targets x 1e5 sources, several
+    threads per target) and tall (3000 targets x 400 sources), against the oracle's FP64
+    direct sums at every target.  Bar: 1e-12 ||c_t||_1 per column."""
+    from nufht_b200 import _lib as L
+    lib = L.lib()
+    rng = np.random.default_rng(int(nu) + (0 if shape == "thin" else 1000))
+    if shape == "thin":
+        m, n = 100_000, 48
+    else:
+        m, n = 400, 3000
+    r = np.sort(300.0 * (1.0 - rng.random(m)))
+    k = np.sort(0.05 + 0.95 * rng.random(n))
+    B = 5
+    c = np.asfortranarray(rng.standard_normal((m, B)))
+    g = np.zeros((n, B), order="F")
+    lib.add_dir_batch(L.dptr(g), nu, L.dptr(r), L.dptr(c), L.dptr(k), m, n, B, m, n)
+    gd = orc.direct_sum(nu, r, k, c, np.arange(n))
+    assert col_err(g, gd, c).max() <= 1e-12, (nu, shape)
+
+
 def test_launch_counter_moves(cuda):
     from nufht_b200 import _lib as L
     from nufht_b200 import _pynufht as pn
@@ -314,3 +338,44 @@ def test_pynufht_plan_cache(cuda, orc):
     assert len(pn._plans.entries) == 3
     pn.clear_plan_cache()
     assert not pn._plans.entries
+
+
+def test_reference_c_program(cuda, orc, tmp_path):
+    """The reference's own C test (src/test_nufht.c: nu = 1/2, f = (1 + r^2)^-n for n = 2, 3
+    on 10000 Gauss-Legendre nodes in [0, 10], 100 k in (0, 10], tol 1e-8), compiled unchanged
+    against the reference header and linked with libnufht_b200.so, runs on the GPU: its
+    printed transform values agree with the oracle on the same inputs, and its errors against
+    the analytic transforms are the oracle's (the truncation of the integral at r = 10)."""
+    import subprocess
+    from test_planner_abi import REF_OUT, write_gl_file
+    exe = os.path.join(REF_OUT, "test_nufht_ref")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref was built without the reference tree")
+    gl = str(tmp_path / "gl10000")
+    write_gl_file(gl)
+    out = subprocess.run([exe, gl], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    cols, cur = {}, None
+    for ln in out.stdout.splitlines():
+        if ln.startswith("# Batch column n="):
+            cur = int(ln.split("=")[1])
+            cols[cur] = []
+        elif ln.strip() and not ln.startswith("#"):
+            cols[cur].append([float(v) for v in ln.split()])
+    assert sorted(cols) == [2, 3]
+    # the same inputs as the program (src/test_nufht.c:47-88)
+    x, w = np.loadtxt(gl, unpack=True)
+    r, w = 5.0 * (x + 1.0), 5.0 * w
+    c = np.stack([r ** 1.5 * (1 + r * r) ** -n * w for n in (2, 3)], axis=1)
+    k = 10.0 * np.arange(1, 101) / 100
+    g = orc.nufht_batch(0.5, r, k, c, 1e-8)
+    for b, n in enumerate((2, 3)):
+        a = np.array(cols[n])
+        assert a.shape == (100, 4) and np.allclose(a[:, 0], k, rtol=1e-7)
+        numeric_oracle = np.sqrt(np.pi / (2 * k)) * g[:, b]
+        l1 = np.abs(c[:, b]).sum()
+        # values are printed with 9 significant digits
+        bound = 1e-8 * np.sqrt(np.pi / (2 * k)) * l1 + 1e-8 * np.abs(numeric_oracle)
+        assert (np.abs(a[:, 2] - numeric_oracle) <= bound).all(), n
+        err_oracle = np.abs(numeric_oracle - a[:, 1]).max()
+        assert np.abs(a[:, 2] - a[:, 1]).max() <= err_oracle + 1e-7, (n, err_oracle)

@@ -45,6 +45,45 @@ def test_struct_layouts_match_reference():
     assert L.NufhtPlan.tables_loaded.offset == 648
 
 
+REF_OUT = os.path.join(ROOT, "oracle", "_ref")
+
+
+def test_c_header_layouts_match_reference_header():
+    """include/nufht_b200.h against the reference's own src/fast_hankel_nufht.h, in C: the
+    build compiles oracle/abi_layout.c against each header, and the checking program only
+    compiles when every struct size and field offset is equal (_Static_assert)."""
+    import subprocess
+    exe = os.path.join(REF_OUT, "abi_layout_check")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref was built without the reference tree")
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=30)
+    assert out.returncode == 0 and "matches the reference header: 47" in out.stdout, out.stdout
+
+
+def write_gl_file(path, n=10000):
+    """Gauss-Legendre nodes and weights on [-1, 1] in the reference's two-column data format
+    (data/gl10000), computed with NumPy."""
+    x, w = np.polynomial.legendre.leggauss(n)
+    np.savetxt(path, np.c_[x, w], fmt="%.17e")
+
+
+def test_reference_c_program_links_the_library(tmp_path):
+    """The reference's src/test_nufht.c, compiled unchanged against its own header and linked
+    with libnufht_b200.so, plans through the drop-in (nufht_plan_init, nufht_scratch_init) and
+    reaches nufht_batch, which reports that there is no GPU here (the GPU test runs it)."""
+    import subprocess
+    from conftest import gpu_available
+    exe = os.path.join(REF_OUT, "test_nufht_ref")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref was built without the reference tree")
+    if gpu_available():
+        pytest.skip("a GPU is present: covered by test_gpu_parity.py::test_reference_c_program")
+    gl = str(tmp_path / "gl10000")
+    write_gl_file(gl)
+    out = subprocess.run([exe, gl], capture_output=True, text=True, timeout=120)
+    assert "nufht_batch returned %d" % -422 in out.stderr, (out.stdout[-500:], out.stderr[-500:])
+
+
 def test_default_options(plib):
     o = plib.nufht_default_options()
     assert o.tol == 1e-8 and o.max_levels == 0 and o.min_dim_prod == 10000

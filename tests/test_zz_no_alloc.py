@@ -64,3 +64,30 @@ def test_noalloc_rejects_oversized_call_without_touching_output(cuda):
     torch.cuda.synchronize()
     assert ret == L.NUFHT_E_TOO_LARGE
     assert bool((g == 7.0).all())
+
+
+def test_noalloc_rejects_host_buffers_and_signs_negative_odd_orders(cuda, orc):
+    """Buffers must be device memory of the current device (a host array is refused before
+    any launch); a negative odd order adds the negated expansion (J_{-n} = (-1)^n J_n)."""
+    import torch
+    from nufht_b200 import _lib as L
+    lib = L.lib()
+    rc, z, ka, K, coef = orc.plan_params(3.0, 1e-8)
+    m, n, B = 3000, 2000, 3
+    r, k, c, g0 = _inputs(7, m, n, B, z)
+    d = lambda a: torch.tensor(a, dtype=torch.float64, device=cuda).contiguous()
+    rd, kd, cd = d(r), d(k), d(c)
+    host_g = np.ascontiguousarray(g0)
+    ret = lib.nufht_b200_add_loc_batch_noalloc(host_g.ctypes.data_as(ctypes.c_void_p), 3.0, _ptr(rd), _ptr(cd),
+                                               _ptr(kd), m, n, K, B, m, n, None)
+    assert ret == -400 and np.array_equal(host_g, g0)
+    gp, gm = d(g0), d(g0)
+    assert lib.nufht_b200_add_loc_batch_noalloc(_ptr(gp), 3.0, _ptr(rd), _ptr(cd), _ptr(kd), m, n, K, B, m, n,
+                                                None) == 0
+    torch.cuda.synchronize()
+    assert lib.nufht_b200_add_loc_batch_noalloc(_ptr(gm), -3.0, _ptr(rd), _ptr(cd), _ptr(kd), m, n, K, B, m, n,
+                                                None) == 0
+    torch.cuda.synchronize()
+    base = d(g0)
+    err = ((gm - base) + (gp - base)).abs().max(dim=1).values.cpu().numpy() / np.abs(c).sum(axis=1)
+    assert err.max() <= 1e-13
