@@ -211,6 +211,15 @@ void nufht_b200_plan_destroy(NufhtDevicePlan *plan);
  * Returns the total number of boxes. */
 long nufht_b200_plan_boxes(const NufhtDevicePlan *plan, int *out, long cap);
 
+/* Replaces generate_boxes (src/fast_hankel_nufht.c:578-744) computed on the GPU: the same
+ * boxes in the same order, from sorted grids in host or device memory (validated on the
+ * device first: NUFHT_E_UNSORTED_RS / _WS).  The lists in `out` are host memory, released
+ * with boxes_free.  nufht_b200_plan_create partitions this way unless the environment sets
+ * NUFHT_B200_HOST_PLANNER=1.  Returns 0 or a negative code. */
+int nufht_b200_generate_boxes_device(const double *rs, int m, const double *ws, int n,
+                                     double z_split, int max_levels, int min_dim_prod,
+                                     int K_loc_threshold, Boxes *out);
+
 /* Human-readable text for any code returned by this library. */
 const char *nufht_b200_strerror(int code);
 
@@ -236,7 +245,9 @@ int nufht_b200_phase_times(double *ms, int nphase);
  * interpolation, FFT flops per vector, expansion terms (2 (K_asy + 1)), K_loc + 1,
  * asymptotic boxes oversampled below 2, 1 if the asymptotic boxes run in FP32 (mixed
  * precision) else 0, and the modelled worst-case error of FP32 asymptotic boxes per unit
- * ||c||_1 (mixed precision is used only where it is at most tol / 4). */
+ * ||c||_1 (mixed precision is used only where it is at most tol / 4); out[15..17] the
+ * planning time in ms (grid validation and box partition, work lists, device tables and
+ * uploads) and out[18] 1 when the partition ran on the device. */
 int nufht_b200_plan_stats(const NufhtDevicePlan *plan, double *out, int n);
 
 /* Measured FP64 fused-multiply-add throughput of the current device (TFLOP/s). */
@@ -296,7 +307,8 @@ int nufht_b200_batch_create(NufhtB200Batch **out, const NufhtB200BatchItem *item
 /* A batch keeps every plan it uses alive (destroying a plan's handle while a batch uses it
  * is safe) and pins it: while pinned, running the plan on its own at a larger width gives
  * it new workspace buffers and leaves the ones the graph recorded allocated until the last
- * batch using the plan is destroyed.  Items may share a plan at different widths. */
+ * batch using the plan is destroyed.  Items may share a plan at different widths.
+ * Creation synchronizes the device (it first runs every item once on its own stream). */
 /* One graph launch on `stream` (a cudaStream_t; asynchronous). */
 int nufht_b200_batch_launch(NufhtB200Batch *batch, void *stream);
 /* Branch count in use, the tuned graph time (ms, 0 when branches was given) and the

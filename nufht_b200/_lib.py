@@ -133,6 +133,9 @@ def _declare(lib):
                                                  ctypes.POINTER(ctypes.c_long)]),
         "nufht_b200_batch_destroy": (None, [vp]),
         "nufht_b200_plan_buffers": (ctypes.c_int, [vp, ctypes.POINTER(vp), c_int_p, c_int_p]),
+        "nufht_b200_generate_boxes_device": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_double,
+                                                            ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                            ctypes.POINTER(Boxes)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

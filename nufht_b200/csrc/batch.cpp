@@ -205,6 +205,9 @@ int nufht_b200_batch_create(NufhtB200Batch** out, const NufhtB200BatchItem* item
   if (cudaSetDevice(device) != cudaSuccess) return NUFHT_E_CUDA;
   int rc = ensure_streams(b.get(), 1);
   if (rc) return rc;
+  // The warm-up below runs the plans on the batch's own stream: work the caller queued on
+  // these plans elsewhere (any stream) must have finished, or the two would share a workspace.
+  if (cudaDeviceSynchronize() != cudaSuccess) return NUFHT_E_CUDA;
   // One ordinary pass first, widest items first: sizes every workspace for its plan's widest
   // item, makes the FFT plans of every width and sets kernel attributes, so that nothing
   // allocates while the graph is captured (items that share a plan may differ in width).

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -134,12 +135,63 @@ void choose_path(DevicePlan* D, int min_dim_prod) {
   }
 }
 
+double wall_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
 int finish_device_plan(DevicePlan* D, int device) {
   D->device = device;
   D->nu2 = (int)std::llround(2.0 * std::fabs(D->P.nu));
   D->sign = (D->P.nu < 0.0 && hankel::is_odd_integer(D->P.nu)) ? -1.0 : 1.0;
+  const double t0 = wall_ms();
   D->build_lists();
-  return D->upload_all();
+  const double t1 = wall_ms();
+  const int rc = D->upload_all();
+  D->plan_ms[1] = t1 - t0;
+  D->plan_ms[2] = wall_ms() - t1;
+  return rc;
+}
+
+// The partition runs on the device unless NUFHT_B200_HOST_PLANNER=1 (the host planner then
+// gives the same boxes; the tests compare the two).
+bool use_device_planner() {
+  const char* e = std::getenv("NUFHT_B200_HOST_PLANNER");
+  return !(e && e[0] == '1');
+}
+
+// Grids of a device plan: device copies (uploaded from host pointers or copied from device
+// pointers), validated and partitioned on the device, plus the host copies the work lists
+// are built from.  Fills D->h_rs, D->h_ws, D->d_rs, D->d_ws and hb.
+int device_grids_and_boxes(DevicePlan* D, const double* rs, const double* ws, const NufhtOptions& opt,
+                           HBoxes* hb) {
+  const int m = D->m, n = D->n;
+  const double t0 = wall_ms();
+  int rc;
+  if ((rc = host_copy(rs, m, &D->h_rs)) || (rc = host_copy(ws, n, &D->h_ws))) return rc;
+  const int Kthr = D->P.K_loc < 0 ? 0 : D->P.K_loc;
+  if (!use_device_planner()) {
+    if (hankel::check_grid(D->h_rs.data(), m)) return NUFHT_E_UNSORTED_RS;
+    if (hankel::check_grid(D->h_ws.data(), n)) return NUFHT_E_UNSORTED_WS;
+    hankel::make_boxes(D->h_rs.data(), m, D->h_ws.data(), n, D->P.z_split, opt.max_levels, opt.min_dim_prod,
+                       Kthr, hb);
+    D->plan_ms[0] = wall_ms() - t0;
+    return 0;
+  }
+  if (cudaMalloc((void**)&D->d_rs, sizeof(double) * (size_t)m) != cudaSuccess ||
+      cudaMalloc((void**)&D->d_ws, sizeof(double) * (size_t)n) != cudaSuccess)
+    return NUFHT_E_CUDA;
+  if (cudaMemcpy(D->d_rs, D->h_rs.data(), sizeof(double) * m, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(D->d_ws, D->h_ws.data(), sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+    return NUFHT_E_CUDA;
+  if ((rc = hankel::device_check_grid(D->d_rs, m, 0)) != 0) return rc == -1 ? NUFHT_E_UNSORTED_RS : rc;
+  if ((rc = hankel::device_check_grid(D->d_ws, n, 0)) != 0) return rc == -1 ? NUFHT_E_UNSORTED_WS : rc;
+  if ((rc = hankel::device_make_boxes(D->d_rs, m, D->d_ws, n, D->P.z_split, opt.max_levels, opt.min_dim_prod,
+                                      Kthr, hb, 0)))
+    return rc;
+  D->partition_on_device = 1;
+  D->plan_ms[0] = wall_ms() - t0;
+  return 0;
 }
 
 // ---- registry of device state for reference-style plans (NufhtPlan has no spare field)
@@ -651,12 +703,9 @@ int nufht_b200_plan_create(NufhtDevicePlan** out, double nu, const double* rs, i
   // regardless of it (NUFHT_B200_MIXED_AVERAGED), else in FP64; always FP64 below 1e-9.
   D->mixed_asy = (flags & (NUFHT_B200_MIXED | NUFHT_B200_MIXED_AVERAGED)) != 0 && D->P.tol >= 1e-9;
   D->mixed_averaged = (flags & NUFHT_B200_MIXED_AVERAGED) != 0;
-  if ((rc = host_copy(rs, m, &D->h_rs)) || (rc = host_copy(ws, n, &D->h_ws))) return rc;
-  if (hankel::check_grid(D->h_rs.data(), m)) return NUFHT_E_UNSORTED_RS;
-  if (hankel::check_grid(D->h_ws.data(), n)) return NUFHT_E_UNSORTED_WS;
   HBoxes hb;
-  hankel::make_boxes(D->h_rs.data(), m, D->h_ws.data(), n, D->P.z_split, opt.max_levels,
-                    opt.min_dim_prod, D->P.K_loc < 0 ? 0 : D->P.K_loc, &hb);
+  D->device = device;
+  if ((rc = device_grids_and_boxes(D.get(), rs, ws, opt, &hb))) return rc;
   D->plan_loc = hb.loc;
   D->plan_asy = hb.asy;
   D->plan_dir = hb.dir;
@@ -665,6 +714,50 @@ int nufht_b200_plan_create(NufhtDevicePlan** out, double nu, const double* rs, i
   NufhtDevicePlan* h = new NufhtDevicePlan;
   h->dp = std::move(D);
   *out = h;
+  return 0;
+}
+
+int nufht_b200_generate_boxes_device(const double* rs, int m, const double* ws, int n, double z_split,
+                                     int max_levels, int min_dim_prod, int K_loc_threshold, Boxes* out) {
+  if (!out) return -200;
+  std::memset(out, 0, sizeof(*out));
+  if (!rs || !ws || m <= 0 || n <= 0) return -200;
+  if (!has_device()) return NUFHT_E_NO_DEVICE;
+  int rc;
+  // device grids are used where they are; host grids are uploaded
+  const double* dr = rs;
+  const double* dw = ws;
+  double *ur = nullptr, *uw = nullptr;
+  auto release = [&]() {
+    cudaFree(ur);
+    cudaFree(uw);
+  };
+  if (!is_device_ptr(rs)) {
+    if (cudaMalloc((void**)&ur, sizeof(double) * (size_t)m) != cudaSuccess ||
+        cudaMemcpy(ur, rs, sizeof(double) * m, cudaMemcpyHostToDevice) != cudaSuccess) {
+      release();
+      return NUFHT_E_CUDA;
+    }
+    dr = ur;
+  }
+  if (!is_device_ptr(ws)) {
+    if (cudaMalloc((void**)&uw, sizeof(double) * (size_t)n) != cudaSuccess ||
+        cudaMemcpy(uw, ws, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess) {
+      release();
+      return NUFHT_E_CUDA;
+    }
+    dw = uw;
+  }
+  HBoxes hb;
+  rc = hankel::device_check_grid(dr, m, 0);
+  if (rc == 0) rc = hankel::device_check_grid(dw, n, 0) == 0 ? 0 : NUFHT_E_UNSORTED_WS;
+  else if (rc == -1) rc = NUFHT_E_UNSORTED_RS;
+  if (rc == 0) rc = hankel::device_make_boxes(dr, m, dw, n, z_split, max_levels, min_dim_prod, K_loc_threshold, &hb, 0);
+  release();
+  if (rc) return rc;
+  out->loc = to_boxvec(hb.loc);
+  out->asy = to_boxvec(hb.asy);
+  out->dir = to_boxvec(hb.dir);
   return 0;
 }
 

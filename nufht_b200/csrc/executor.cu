@@ -27,6 +27,7 @@
 #include "kernels_asy.cuh"
 #include "kernels_dir.cuh"
 #include "kernels_loc.cuh"
+#include "kernels_loc_mma.cuh"
 
 namespace hankel {
 
@@ -35,6 +36,13 @@ std::atomic<long long> g_launch_counter{0};
 // Optional per-phase device timing: CUDA events recorded on the launching stream around
 // each phase of run(); read (and released) by phase_times().
 std::atomic<bool> g_phase_timing{false};
+
+// Local boxes on the SIMT kernels instead of the tensor-core ones (NUFHT_B200_LOC_SIMT=1; the
+// tests compare the two forms).
+const bool g_loc_simt = [] {
+  const char* e = std::getenv("NUFHT_B200_LOC_SIMT");
+  return e && e[0] == '1';
+}();
 
 namespace {
 
@@ -140,6 +148,33 @@ double fp32_error_bound(const DevicePlan& D, double kappa) {
   return err;
 }
 
+// Wimp degree the local boxes need.  Term l of the expansion is b_l(z) C_l with
+// |b_l(z)| <= |J_{l0+odd+l}(z)| <= (z/2)^n / n!  (n = l0+odd+l; |J_m| <= 1) and
+// |C_l| <= 2 ||c||_1 (|T_l| <= 1, weight <= 2), so all terms from l = L+1 on add at most
+//   2 ||c||_1 sum_{n >= n0} (z/2)^n / n!  <=  2 ||c||_1 (z/2)^n0 / n0! / (1 - z / (2 (n0+1))),
+// n0 = l0+odd+L+1, at the largest z = k r_end / 2 of any local box.  The degree is the
+// table's K_loc, lowered to the smallest L whose tail stays below 1e-3 tol ||c||_1 (large
+// orders: K_loc = 551 at nu = 100, tol 1e-8, while z < 80 needs about 80 terms).
+int wimp_degree_needed(const PlanParams& P, const std::vector<HBox>& boxes, const double* rs, const double* ws) {
+  const int K = P.K_loc;
+  if (K <= 0 || boxes.empty()) return std::max(K, 0);
+  double zmax = 0.0;
+  for (const HBox& hb : boxes) zmax = std::max(zmax, ws[hb.i1] * rs[hb.j1] / 2.0);
+  if (!(zmax > 0.0)) return 0;
+  const int nu_int = (int)std::llround(std::fabs(P.nu));
+  const int base = nu_int / 2 + (nu_int & 1);  // l0 + odd
+  const double lh = std::log(zmax / 2.0);
+  const double target = std::log(1e-3 * P.tol / 2.0);
+  for (int L = 0; L < K; ++L) {
+    const int n0 = base + L + 1;
+    const double q = zmax / (2.0 * (n0 + 1.0));
+    if (q >= 1.0) continue;
+    const double lt = n0 * lh - std::lgamma(n0 + 1.0) - std::log1p(-q);
+    if (lt <= target) return L;
+  }
+  return K;
+}
+
 // Kernel shape for oversampling sigma and width W: beta = 2.30 W at sigma = 2 (the
 // value of Barnett, Magland & af Klinteberg 2019), 0.97 pi (1 - 1/(2 sigma)) W otherwise.
 double es_beta(double sigma, int W) {
@@ -213,7 +248,8 @@ void DevicePlan::build_lists() {
   locb.clear();
   proj.clear();
   eval.clear();
-  KL1 = P.K_loc + 1;
+  K_eval = wimp_degree_needed(P, loc_boxes, rs, ws);
+  KL1 = K_eval + 1;
   for (size_t b = 0; b < loc_boxes.size(); ++b) {
     const HBox& hb = loc_boxes[b];
     LocBoxD d;
@@ -474,15 +510,31 @@ void DevicePlan::build_lists() {
 
 int DevicePlan::upload_all() {
   NUFHT_CUDA_TRY(cudaSetDevice(device));
-  NUFHT_CUDA_TRY(cudaMalloc((void**)&d_rs, sizeof(double) * (size_t)m));
-  NUFHT_CUDA_TRY(cudaMalloc((void**)&d_ws, sizeof(double) * (size_t)n));
-  NUFHT_CUDA_TRY(cudaMemcpy(d_rs, h_rs.data(), sizeof(double) * m, cudaMemcpyHostToDevice));
-  NUFHT_CUDA_TRY(cudaMemcpy(d_ws, h_ws.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+  if (!d_rs) {  // the device planner uploads the grids first
+    NUFHT_CUDA_TRY(cudaMalloc((void**)&d_rs, sizeof(double) * (size_t)m));
+    NUFHT_CUDA_TRY(cudaMemcpy(d_rs, h_rs.data(), sizeof(double) * m, cudaMemcpyHostToDevice));
+  }
+  if (!d_ws) {
+    NUFHT_CUDA_TRY(cudaMalloc((void**)&d_ws, sizeof(double) * (size_t)n));
+    NUFHT_CUDA_TRY(cudaMemcpy(d_ws, h_ws.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+  }
   int rc;
   if ((rc = upload(locb, &d_locb)) || (rc = upload(proj, &d_proj)) || (rc = upload(eval, &d_eval)) ||
       (rc = upload(dir, &d_dir)) || (rc = upload(asyb, &d_asyb)) || (rc = upload(spread, &d_spread)) ||
       (rc = upload(interp, &d_interp)))
     return rc;
+  // J_nu table for the direct boxes where J_nu costs a recurrence over the order (integer
+  // orders from 2, half-integer orders from 3/2) and their arguments k r stay below the
+  // table's reach; larger arguments are evaluated directly.
+  if (!dir.empty() && nu2 >= 3) {
+    double xmax = 0.0;
+    for (const DirItem& it : dir) xmax = std::max(xmax, h_ws[it.i0 + it.ni - 1] * h_rs[it.j0 + it.nj - 1]);
+    jtab_n = (int)std::min<double>(std::ceil(xmax) + 1.0, (double)kJTabMaxIntervals);
+    NUFHT_CUDA_TRY(cudaMalloc((void**)&d_jtab, sizeof(double) * (size_t)jtab_n * kJTabCoefs));
+    k_build_jtable<<<jtab_n, kJTabCoefs>>>(nu2, d_jtab, jtab_n);
+    NUFHT_LAUNCH_CHECK();
+    NUFHT_CUDA_TRY(cudaDeviceSynchronize());
+  }
   if (!asyb.empty()) {
     if (NLP > kMaxNLP) return NUFHT_E_TOO_LARGE;
     NUFHT_CUDA_TRY(cudaMalloc((void**)&d_corr, sizeof(double) * (size_t)total_corr));
@@ -539,7 +591,7 @@ DevicePlan::~DevicePlan() {
   release_fft();
   cudaFree(d_rs); cudaFree(d_ws); cudaFree(d_locb); cudaFree(d_proj); cudaFree(d_eval);
   cudaFree(d_dir); cudaFree(d_asyb); cudaFree(d_spread); cudaFree(d_interp);
-  cudaFree(d_corr); cudaFree(d_post);
+  cudaFree(d_corr); cudaFree(d_post); cudaFree(d_jtab);
   cudaFree(d_grid); cudaFree(d_partial); cudaFree(d_cheb); cudaFree(d_fft_work);
   for (void* p : retired) cudaFree(p);
   cudaFree(d_stage_c); cudaFree(d_stage_g); cudaFree(d_stage_t);
@@ -646,7 +698,8 @@ template <int BT>
 int launch_dir(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B,
                cudaStream_t st, double sgn) {
   dim3 g((unsigned)D.dir.size(), (unsigned)((B + BT - 1) / BT));
-  k_dir<BT><<<g, kDirThreads, 0, st>>>(D.d_rs, D.d_ws, cs, ld_cs, gs, ld_gs, B, D.d_dir, D.nu2, sgn);
+  k_dir<BT><<<g, kDirThreads, 0, st>>>(D.d_rs, D.d_ws, cs, ld_cs, gs, ld_gs, B, D.d_dir, D.nu2, sgn, D.d_jtab,
+                                       D.jtab_n);
   NUFHT_LAUNCH_CHECK();
   return 0;
 }
@@ -667,46 +720,127 @@ int launch_loc_eval_t(const double* ws, double* gs, int ld_gs, int B, const LocB
   return 0;
 }
 
+// Projection on the FP64 tensor cores (k_loc_proj_mma): columns per CTA and staged sources
+// per round chosen so that the output tiles fit the warps' registers and the tables the
+// shared-memory budget.  Returns 1 when the degree is too large for it (SIMT path then).
+int launch_loc_proj_mma(const double* rs, const double* cs, int ld_cs, int B, const LocBoxD* d_box,
+                        const ProjItem* d_proj, int nproj, double* d_partial, int KL1, int odd, cudaStream_t st) {
+  const int nmt = round8(KL1) / 8;
+  int BT = std::min(32, round8(B));
+  while (BT > 8 && nmt * (BT / 8) > kLocMmaWarps * 4) BT -= 8;
+  const int tiles = nmt * (BT / 8);
+  if (tiles > kLocMmaWarps * 16) return 1;
+  int chunk = 128;
+  LocProjMma L = loc_proj_mma_layout(KL1, BT, chunk);
+  while (chunk > 4 && L.doubles() > kLocSmemDoubles) {
+    chunk -= 4;
+    L = loc_proj_mma_layout(KL1, BT, chunk);
+  }
+  if (L.doubles() > kLocSmemDoubles) return 1;
+  const size_t sm = sizeof(double) * L.doubles();
+  dim3 g((unsigned)nproj, (unsigned)((B + BT - 1) / BT));
+  if (tiles <= kLocMmaWarps * 4) {
+    if (sm > 48 * 1024) cudaFuncSetAttribute(k_loc_proj_mma<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_loc_proj_mma<4><<<g, kLocThreads, sm, st>>>(rs, cs, ld_cs, B, d_box, d_proj, KL1, odd, d_partial, BT, L);
+  } else {
+    if (sm > 48 * 1024) cudaFuncSetAttribute(k_loc_proj_mma<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_loc_proj_mma<16><<<g, kLocThreads, sm, st>>>(rs, cs, ld_cs, B, d_box, d_proj, KL1, odd, d_partial, BT, L);
+  }
+  NUFHT_LAUNCH_CHECK();
+  return 0;
+}
+
+// Evaluation on the FP64 tensor cores (k_loc_eval_mma): the largest tile of targets (128,
+// 32, 16 or 8) whose Bessel table fits in 100 KB of shared memory (two CTAs per SM), else
+// the largest that fits at all.  Returns 1 when even 8 targets do not fit.
+template <int TI>
+int launch_loc_eval_mma_t(const double* ws, double* gs, int ld_gs, int B, const LocBoxD* d_box, const EvalItem* d_eval,
+                          int neval, const double* d_cheb, int K, int nu_int, double sgn, const LocEvalMma& L,
+                          cudaStream_t st) {
+  const size_t sm = sizeof(double) * L.doubles();
+  if (sm > 48 * 1024) cudaFuncSetAttribute(k_loc_eval_mma<TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_loc_eval_mma<TI><<<(unsigned)neval, kLocThreads, sm, st>>>(ws, gs, ld_gs, B, d_box, d_eval, d_cheb, K, nu_int, sgn,
+                                                               L);
+  NUFHT_LAUNCH_CHECK();
+  return 0;
+}
+
+int launch_loc_eval_mma(const double* ws, double* gs, int ld_gs, int B, const LocBoxD* d_box, const EvalItem* d_eval,
+                        int neval, const double* d_cheb, int K, int nu_int, double sgn, cudaStream_t st) {
+  const int maxo = nu_int / 2 + K + (nu_int & 1);
+  // The tile with the most targets resident per SM (shared memory decides how many CTAs
+  // fit); ties go to the larger tile, which stages the coefficients for more targets.
+  const int tis[4] = {128, 32, 16, 8};
+  int pick = -1, best = 0;
+  for (int q = 0; q < 4; ++q) {
+    const size_t bytes = sizeof(double) * loc_eval_mma_layout(tis[q], maxo).doubles();
+    if (bytes > sizeof(double) * kLocSmemDoubles) continue;
+    const int per_sm = tis[q] * (int)std::min<size_t>(8, (size_t)(224 * 1024) / (bytes + 1024));
+    if (per_sm > best) {
+      best = per_sm;
+      pick = tis[q];
+    }
+  }
+  if (pick < 0) return 1;
+  const LocEvalMma L = loc_eval_mma_layout(pick, maxo);
+  switch (pick) {
+    case 128: return launch_loc_eval_mma_t<128>(ws, gs, ld_gs, B, d_box, d_eval, neval, d_cheb, K, nu_int, sgn, L, st);
+    case 32: return launch_loc_eval_mma_t<32>(ws, gs, ld_gs, B, d_box, d_eval, neval, d_cheb, K, nu_int, sgn, L, st);
+    case 16: return launch_loc_eval_mma_t<16>(ws, gs, ld_gs, B, d_box, d_eval, neval, d_cheb, K, nu_int, sgn, L, st);
+    default: return launch_loc_eval_mma_t<8>(ws, gs, ld_gs, B, d_box, d_eval, neval, d_cheb, K, nu_int, sgn, L, st);
+  }
+}
+
 // The local-expansion kernels over `nbox` boxes (g += their contribution): projection per
 // source chunk, reduction of the partial projections per box, evaluation at the targets.
+// Both contractions run on the FP64 tensor cores; the SIMT kernels remain for Wimp degrees
+// beyond their tile limits.
 int launch_loc(const double* rs, const double* ws, const double* cs, int ld_cs, double* gs, int ld_gs, int B,
                const LocBoxD* d_box, int nbox, const ProjItem* d_proj, int nproj, const EvalItem* d_eval, int neval,
                double* d_partial, double* d_cheb, int K, int nu_int, double sgn, cudaStream_t st) {
   const int KL1 = K + 1;
   const int maxo = nu_int / 2 + K + (nu_int & 1);
   if (KL1 > kLocThreads * kLocMaxNL || maxo > 2304) return NUFHT_E_TOO_LARGE;
-  // columns per projection CTA: the widest power of two (<= 32, <= B) for which each thread
-  // owns one order, or, for very large degrees, at most kLocMaxNL orders
-  const int cap = KL1 <= kLocThreads ? kLocThreads : kLocThreads * kLocMaxNL;
-  int BT = 32;
-  while (BT > 1 && KL1 * BT > cap) BT >>= 1;
-  BT = std::max(1, std::min(BT, B));
-  const int LS = kLocThreads / BT;
-  const int NL = (KL1 + LS - 1) / LS;
-  if (NL > kLocMaxNL) return NUFHT_E_TOO_LARGE;
-  // sources per staging round: even (the projection reads the table in 16-byte pairs)
-  const int chunk = (int)std::min<size_t>(kLocChunk, kLocSmemDoubles / (size_t)(KL1 + BT)) & ~1;
-  if (chunk < 2) return NUFHT_E_TOO_LARGE;
-  const size_t sm = sizeof(double) * ((size_t)KL1 * chunk + (size_t)chunk * BT);
-  dim3 g((unsigned)nproj, (unsigned)((B + BT - 1) / BT));
   {
     PhaseScope ps(kPhaseLocProj, st);
-    if (NL == 1) {
-      if (sm > 48 * 1024) cudaFuncSetAttribute(k_loc_proj<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      k_loc_proj<1><<<g, kLocThreads, sm, st>>>(rs, cs, ld_cs, B, d_box, d_proj, KL1, nu_int & 1, d_partial, BT,
-                                               chunk);
-    } else {
-      if (sm > 48 * 1024)
-        cudaFuncSetAttribute(k_loc_proj<kLocMaxNL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      k_loc_proj<kLocMaxNL><<<g, kLocThreads, sm, st>>>(rs, cs, ld_cs, B, d_box, d_proj, KL1, nu_int & 1,
-                                                        d_partial, BT, chunk);
+    int rc = g_loc_simt ? 1 : launch_loc_proj_mma(rs, cs, ld_cs, B, d_box, d_proj, nproj, d_partial, KL1, nu_int & 1, st);
+    if (rc < 0) return rc;
+    if (rc == 1) {
+      // columns per projection CTA: the widest power of two (<= 32, <= B) for which each
+      // thread owns one order, or, for very large degrees, at most kLocMaxNL orders
+      const int cap = KL1 <= kLocThreads ? kLocThreads : kLocThreads * kLocMaxNL;
+      int BT = 32;
+      while (BT > 1 && KL1 * BT > cap) BT >>= 1;
+      BT = std::max(1, std::min(BT, B));
+      const int LS = kLocThreads / BT;
+      const int NL = (KL1 + LS - 1) / LS;
+      if (NL > kLocMaxNL) return NUFHT_E_TOO_LARGE;
+      // sources per staging round: even (the projection reads the table in 16-byte pairs)
+      const int chunk = (int)std::min<size_t>(kLocChunk, kLocSmemDoubles / (size_t)(KL1 + BT)) & ~1;
+      if (chunk < 2) return NUFHT_E_TOO_LARGE;
+      const size_t sm = sizeof(double) * ((size_t)KL1 * chunk + (size_t)chunk * BT);
+      dim3 g((unsigned)nproj, (unsigned)((B + BT - 1) / BT));
+      if (NL == 1) {
+        if (sm > 48 * 1024) cudaFuncSetAttribute(k_loc_proj<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_loc_proj<1><<<g, kLocThreads, sm, st>>>(rs, cs, ld_cs, B, d_box, d_proj, KL1, nu_int & 1, d_partial, BT,
+                                                 chunk);
+      } else {
+        if (sm > 48 * 1024)
+          cudaFuncSetAttribute(k_loc_proj<kLocMaxNL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_loc_proj<kLocMaxNL><<<g, kLocThreads, sm, st>>>(rs, cs, ld_cs, B, d_box, d_proj, KL1, nu_int & 1,
+                                                          d_partial, BT, chunk);
+      }
+      NUFHT_LAUNCH_CHECK();
     }
-    NUFHT_LAUNCH_CHECK();
     long long tot = (long long)nbox * KL1 * B;
     k_loc_reduce<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_box, nbox, KL1, B, d_partial, d_cheb);
     NUFHT_LAUNCH_CHECK();
   }
   PhaseScope ps(kPhaseLocEval, st);
+  if (!g_loc_simt) {
+    int rc = launch_loc_eval_mma(ws, gs, ld_gs, B, d_box, d_eval, neval, d_cheb, K, nu_int, sgn, st);
+    if (rc <= 0) return rc;
+  }
   if (maxo <= 64) return launch_loc_eval_t<64>(ws, gs, ld_gs, B, d_box, d_eval, neval, d_cheb, K, nu_int, sgn, st);
   if (maxo <= 160) return launch_loc_eval_t<160>(ws, gs, ld_gs, B, d_box, d_eval, neval, d_cheb, K, nu_int, sgn, st);
   if (maxo <= 640) return launch_loc_eval_t<640>(ws, gs, ld_gs, B, d_box, d_eval, neval, d_cheb, K, nu_int, sgn, st);
@@ -730,7 +864,7 @@ int DevicePlan::run(const double* cs, int ld_cs, double* gs, int ld_gs, int B, c
   // ---- local boxes
   if (!locb.empty()) {
     rc = launch_loc(d_rs, d_ws, cs, ld_cs, gs, ld_gs, B, d_locb, (int)locb.size(), d_proj, (int)proj.size(), d_eval,
-                    (int)eval.size(), d_partial, d_cheb, P.K_loc, nu2 / 2, sgn, st);
+                    (int)eval.size(), d_partial, d_cheb, K_eval, nu2 / 2, sgn, st);
     if (rc) return rc;
   }
   // ---- asymptotic boxes

@@ -97,6 +97,7 @@ struct DevicePlan {
 
   // work lists
   int KL1 = 0, W = 0;
+  int K_eval = 0;  // Wimp degree evaluated: K_loc, or fewer where the dropped terms are negligible
   std::vector<LocBoxD> locb;
   std::vector<ProjItem> proj;
   std::vector<EvalItem> eval;
@@ -121,6 +122,8 @@ struct DevicePlan {
   AsyBoxD* d_asyb = nullptr;
   SpreadItem* d_spread = nullptr;
   InterpItem* d_interp = nullptr;
+  double* d_jtab = nullptr;   // J_nu table of the direct boxes (orders whose evaluation is costly)
+  int jtab_n = 0;             // unit intervals of d_jtab: it covers [0, jtab_n)
   double* d_corr = nullptr;   // 1 / psi-hat of the second stage, per box cell
   double2* d_post = nullptr;  // exp(i (phi + k C)) / psi-hat(theta_k), per box target
 
@@ -151,6 +154,11 @@ struct DevicePlan {
   // copy streams and events of the pipelined host-buffer path (created on first use)
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   cudaEvent_t ev_in[4] = {}, ev_done[4] = {};
+
+  // planning cost (host wall-clock ms): validation and box partition, work lists, device
+  // tables and uploads; 1 when the partition ran on the device
+  double plan_ms[3] = {0, 0, 0};
+  int partition_on_device = 0;
 
   std::mutex mu;
 
@@ -203,6 +211,12 @@ int run_asy_f64(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_g
                 double sgn);
 
 int run_besselj(double nu, const double* x, double* out, long count, cudaStream_t st);
+
+// Device planner (planner_dev.cu): validation of a device-resident grid (0, or -1 when not
+// finite, non-negative and non-decreasing) and the box partition from device-resident grids.
+int device_check_grid(const double* d_a, int len, cudaStream_t st);
+int device_make_boxes(const double* d_rs, int m, const double* d_ws, int n, double z, int max_levels,
+                      int min_dim_prod, int Kthr, HBoxes* out, cudaStream_t st);
 
 // out[c * ldo + r] = in[r * ldi + c] for r < rows, c < cols (device pointers): a row-major
 // batch to the executor's column-major one and back.

@@ -34,6 +34,7 @@ constexpr int kChunkSources = 2048; // sources per mode-1 work item, at most
 constexpr int kTileMaxSources = 4096;
 constexpr int kInterpTile = 128;    // targets per interpolation CTA
 constexpr int kInterpChunk = 32;    // targets per shared-memory round
+constexpr int kInterpPrefetch = 8;  // cells between the L1 prefetch of a grid row and its fetch
 
 template <typename T> struct Cplx;
 template <> struct Cplx<double> { using type = double2; };
@@ -188,19 +189,8 @@ __device__ __forceinline__ void load_weights(const double* src, double (&w)[WE])
 }
 
 // acc += w * a for complex w and real a: one packed two-lane FMA in single precision
-// (fma.rn.f32x2, sm_100 and later), two FMAs in double.
-__device__ __forceinline__ void cfma(float2& acc, float2 w, float a) {
-  unsigned long long rd;
-  const unsigned long long rw = (unsigned long long)__float_as_uint(w.x) |
-                                ((unsigned long long)__float_as_uint(w.y) << 32);
-  const unsigned long long ra = (unsigned long long)__float_as_uint(a) |
-                                ((unsigned long long)__float_as_uint(a) << 32);
-  const unsigned long long rc = (unsigned long long)__float_as_uint(acc.x) |
-                                ((unsigned long long)__float_as_uint(acc.y) << 32);
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(rd) : "l"(rw), "l"(ra), "l"(rc));
-  acc.x = __uint_as_float((unsigned)(rd & 0xffffffffull));
-  acc.y = __uint_as_float((unsigned)(rd >> 32));
-}
+// (__ffma2_rn, FFMA2 on sm_100 and later), two FMAs in double.
+__device__ __forceinline__ void cfma(float2& acc, float2 w, float a) { acc = __ffma2_rn(w, make_float2(a, a), acc); }
 __device__ __forceinline__ void cfma(double2& acc, double2 w, double a) {
   acc.x = fma(w.x, a, acc.x);
   acc.y = fma(w.y, a, acc.y);
@@ -460,6 +450,15 @@ __global__ void __launch_bounds__(256) k_asy_interp(
     int idx = cell < 0 ? cell + n2 : (cell >= n2 ? cell - n2 : cell);
     return active ? row[u][idx] : cmake<T>(0, 0);
   };
+  // The ring fetches a cell one step before its stencil needs it, far less than a DRAM
+  // round trip; an L1 prefetch kInterpPrefetch cells further ahead (an address inside the
+  // row, wrapped like the fetch) makes those fetches L1 hits.
+  auto prefetch = [&](int cell, int u) {
+    if (!active) return;
+    int idx = cell % n2;
+    if (idx < 0) idx += n2;
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(row[u] + idx));
+  };
   // Stage targets [k0, k0 + nk) (all threads; barriers on both sides).
   auto stage = [&](int k0, int nk) {
     __syncthreads();
@@ -559,12 +558,17 @@ __global__ void __launch_bounds__(256) k_asy_interp(
       if (nxt == c + 1) {
         // the slot of cell c takes cell c + R (one cell ahead of the next stencil)
 #pragma unroll
-        for (int u = 0; u < LPT; ++u) gw[u][jj] = fetch(c + R, u);
+        for (int u = 0; u < LPT; ++u) {
+          gw[u][jj] = fetch(c + R, u);
+          prefetch(c + R + kInterpPrefetch, u);
+        }
       } else {
 #pragma unroll
         for (int q = 0; q < R; ++q)
 #pragma unroll
           for (int u = 0; u < LPT; ++u) gw[u][(jj + 1 + q) % R] = fetch(nxt + q, u);
+#pragma unroll
+        for (int u = 0; u < LPT; ++u) prefetch(nxt + R + kInterpPrefetch, u);
       }
       c = nxt;
     }

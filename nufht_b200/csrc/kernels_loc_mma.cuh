@@ -1,0 +1,229 @@
+// Local boxes on the FP64 tensor cores: the two contractions of the Wimp expansion
+// (src/expansions.c:212-337) as warp-level DMMA products (mma.sync.aligned.m8n8k4 with
+// FP64 operands and accumulators; sm_100a executes them on its FP64 tensor pipe).
+//
+//   projection  C[l,t] = sum_j T_l(r_j / r_end) c[j,t]      (K+1) x nj  times  nj x B
+//   evaluation  g[i,t] += sum_l b_l(k_i r_end / 2) C[l,t]     ni x (K+1)  times  (K+1) x B
+//
+// Both stage their left operand in shared memory (the Chebyshev table of a source chunk; the
+// Bessel table J_0..J_maxo of a tile of targets, from which b_l is formed while the fragment
+// is loaded) and keep 8 x 8 output tiles in registers.  Shared-memory row strides are chosen
+// == 4 (mod 16) doubles so that the fragment loads of a half-warp (4 rows x 4 consecutive
+// columns) fall in distinct banks.
+#pragma once
+
+#include "kernels_loc.cuh"
+
+namespace hankel {
+
+// d += a * b for one 8 x 8 x 4 tile: lane q holds A[q/4][q%4], B[q%4][q/4] and
+// D[q/4][2(q%4)], D[q/4][2(q%4)+1].
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+__host__ __device__ constexpr int round8(int v) { return (v + 7) & ~7; }
+// Smallest stride >= v with stride == 4 (mod 16).
+__host__ __device__ constexpr int stride4(int v) { return v + ((4 - v) % 16 + 16) % 16; }
+
+constexpr int kLocMmaWarps = kLocThreads / 32;
+
+// Shared-memory layout of k_loc_proj_mma (doubles): the table T[MT8][TS] then c[chunk][BS].
+struct LocProjMma {
+  int MT8, TS, BS, chunk;
+  __host__ __device__ size_t doubles() const { return (size_t)MT8 * TS + (size_t)chunk * BS; }
+};
+inline LocProjMma loc_proj_mma_layout(int KL1, int BT, int chunk) {
+  LocProjMma L;
+  L.MT8 = round8(KL1);
+  L.chunk = chunk;
+  L.TS = stride4(chunk);
+  L.BS = stride4(round8(BT));
+  return L;
+}
+
+// Projection of one source chunk item onto the Chebyshev polynomials, BT columns per CTA.
+// Warp w owns the output tiles w, w + 8, ... (at most NT) of the (MT8/8) x (BT8/8) tile grid.
+template <int NT>
+__global__ void __launch_bounds__(kLocThreads) k_loc_proj_mma(
+    const double* __restrict__ rs, const double* __restrict__ cs, int ld_cs, int B,
+    const LocBoxD* __restrict__ boxes, const ProjItem* __restrict__ items, int KL1, int odd,
+    double* __restrict__ partial, int BT, LocProjMma L) {
+  const ProjItem it = items[blockIdx.x];
+  const LocBoxD bx = boxes[it.box];
+  const int t0 = blockIdx.y * BT;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* sT = reinterpret_cast<double*>(smem_raw);  // [MT8][TS]
+  double* sC = sT + (size_t)L.MT8 * L.TS;              // [chunk][BS]
+  const int chunk = L.chunk;
+  const int nnt = round8(BT) >> 3;
+  const int ntiles = (L.MT8 >> 3) * nnt;
+  double acc[NT][2];
+#pragma unroll
+  for (int q = 0; q < NT; ++q) acc[q][0] = acc[q][1] = 0.0;
+  // padded orders KL1 .. MT8-1 stay zero
+  for (int e = tid; e < (L.MT8 - KL1) * L.TS; e += blockDim.x) sT[(size_t)KL1 * L.TS + e] = 0.0;
+  const double inv_end = bx.r_end > 0.0 ? 1.0 / bx.r_end : 0.0;
+  const int nseg = (KL1 + kLocSeg - 1) / kLocSeg;
+  for (int s0 = 0; s0 < it.nj; s0 += chunk) {
+    const int ns = min(chunk, it.nj - s0);
+    __syncthreads();  // previous chunk consumed
+    for (int e = tid; e < nseg * chunk; e += blockDim.x) {
+      const int sg = e / chunk, s = e - sg * chunk;
+      const int l0 = sg * kLocSeg, l1 = min(KL1, l0 + kLocSeg);
+      if (s < ns) {
+        double x = rs[it.j0 + s0 + s] * inv_end;
+        x = fmin(fmax(x, -1.0), 1.0);
+        const double th = acos(x);
+        const int m0 = odd ? 2 * l0 + 1 : 2 * l0;
+        double tp = cos((double)(m0 - 2) * th);
+        double tc = cos((double)m0 * th);
+        const double two_t2 = 2.0 * (2.0 * x * x - 1.0);
+        for (int l = l0; l < l1; ++l) {
+          sT[(size_t)l * L.TS + s] = (odd || l > 0) ? 2.0 * tc : tc;
+          const double tn = two_t2 * tc - tp;
+          tp = tc;
+          tc = tn;
+        }
+      } else {
+        for (int l = l0; l < l1; ++l) sT[(size_t)l * L.TS + s] = 0.0;
+      }
+    }
+    for (int e = tid; e < chunk * L.BS; e += blockDim.x) {
+      const int s = e / L.BS, tt = e - s * L.BS;
+      sC[e] = (s < ns && tt < BT && t0 + tt < B) ? cs[(size_t)(t0 + tt) * ld_cs + it.j0 + s0 + s] : 0.0;
+    }
+    __syncthreads();
+    const int ar = lane >> 2, ac = lane & 3;
+#pragma unroll
+    for (int q = 0; q < NT; ++q) {
+      const int tile = warp + q * kLocMmaWarps;
+      if (tile < ntiles) {
+        const int mt = tile / nnt, nt = tile - mt * nnt;
+        const double* pa = sT + (size_t)(mt * 8 + ar) * L.TS + ac;
+        const double* pb = sC + (size_t)ac * L.BS + nt * 8 + ar;
+#pragma unroll 4
+        for (int k0 = 0; k0 < chunk; k0 += 4) dmma884(acc[q][0], acc[q][1], pa[k0], pb[(size_t)k0 * L.BS]);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < NT; ++q) {
+    const int tile = warp + q * kLocMmaWarps;
+    if (tile >= ntiles) continue;
+    const int mt = tile / nnt, nt = tile - mt * nnt;
+    const int l = mt * 8 + (lane >> 2);
+    const int tt = nt * 8 + 2 * (lane & 3);
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+      if (l < KL1 && tt + h < BT && t0 + tt + h < B)
+        partial[((size_t)blockIdx.x * KL1 + l) * B + t0 + tt + h] = acc[q][h];
+  }
+}
+
+// Evaluation: each CTA takes one item (<= kLocTargets targets of one box) in tiles of TI
+// targets.  Per tile, TI threads run Miller's recurrence for J_0 .. J_maxo at
+// z = k r_end / 2 into a shared table (one row per target); then the warps form
+// b_l = J_{l0+odd+l} J_{|l-l0|} (-1)^{max(l-l0,0)} while loading the left fragments and
+// multiply by the box's coefficients C, staged kLocMmaK orders x 64 columns at a time.
+constexpr int kLocMmaK = 64;     // orders of C staged per round
+constexpr int kLocMmaCols = 64;  // columns per pass over a tile
+struct LocEvalMma {
+  int TI, JS, CS;
+  __host__ __device__ size_t doubles() const { return (size_t)TI * JS + (size_t)kLocMmaK * CS; }
+};
+inline LocEvalMma loc_eval_mma_layout(int TI, int maxo) {
+  LocEvalMma L;
+  L.TI = TI;
+  L.JS = stride4(maxo + 1);
+  L.CS = stride4(kLocMmaCols);
+  return L;
+}
+
+template <int TI>
+__global__ void __launch_bounds__(kLocThreads) k_loc_eval_mma(
+    const double* __restrict__ ws, double* __restrict__ gs, int ld_gs, int B,
+    const LocBoxD* __restrict__ boxes, const EvalItem* __restrict__ items,
+    const double* __restrict__ cheb, int K, int nu_int, double sgn, LocEvalMma L) {
+  constexpr int MT = TI / 8;                                      // m-tiles per target tile
+  constexpr int NTW = (MT * (kLocMmaCols / 8) + kLocMmaWarps - 1) / kLocMmaWarps;  // tiles per warp
+  const EvalItem it = items[blockIdx.x];
+  const LocBoxD bx = boxes[it.box];
+  const int KL1 = K + 1;
+  const int l0 = nu_int / 2, odd = nu_int & 1;
+  const int maxo = l0 + K + odd;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ar = lane >> 2, ac = lane & 3;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* sJ = reinterpret_cast<double*>(smem_raw);  // [TI][JS]
+  double* sC = sJ + (size_t)TI * L.JS;                 // [kLocMmaK][CS]
+  const double* cbox = cheb + (size_t)it.box * KL1 * B;
+  for (int i0 = 0; i0 < it.ni; i0 += TI) {
+    __syncthreads();  // previous tile's table consumed
+    if (tid < TI) {
+      double* row = sJ + (size_t)tid * L.JS;
+      const int i = it.i0 + i0 + tid;
+      const double z = i0 + tid < it.ni ? ws[i] * bx.r_end / 2.0 : 0.0;
+      if (z < 1e-30) {
+        for (int q = 0; q <= maxo; ++q) row[q] = 0.0;
+        row[0] = 1.0;
+      } else {
+        bessel_j_orders(maxo, z, row);
+      }
+    }
+    for (int cb = 0; cb < B; cb += kLocMmaCols) {
+      const int ncol = min(kLocMmaCols, B - cb);
+      double acc[NTW][2];
+#pragma unroll
+      for (int q = 0; q < NTW; ++q) acc[q][0] = acc[q][1] = 0.0;
+      for (int kc = 0; kc < KL1; kc += kLocMmaK) {
+        const int kn = min(kLocMmaK, KL1 - kc);
+        const int kn4 = (kn + 3) & ~3, nc8 = round8(ncol);
+        __syncthreads();  // table written / previous coefficients consumed
+        for (int e = tid; e < kn4 * nc8; e += blockDim.x) {
+          const int l = e / nc8, t = e - l * nc8;
+          sC[(size_t)l * L.CS + t] = (l < kn && t < ncol) ? cbox[(size_t)(kc + l) * B + cb + t] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < NTW; ++q) {
+          const int tile = warp + q * kLocMmaWarps;
+          if (tile < MT * (kLocMmaCols / 8)) {
+            const int mt = tile / (kLocMmaCols / 8), nt = tile - mt * (kLocMmaCols / 8);
+            if (nt * 8 < ncol) {
+              const double* jrow = sJ + (size_t)(mt * 8 + ar) * L.JS;
+              for (int k0 = 0; k0 < kn; k0 += 4) {
+                const int l = kc + k0 + ac;  // order of this lane's A element
+                double a = 0.0;
+                if (l < KL1) {
+                  const int lo = l > l0 ? l - l0 : l0 - l;
+                  a = jrow[l0 + odd + l] * jrow[lo];
+                  if (l > l0 && ((l - l0) & 1)) a = -a;
+                }
+                const double b = sC[(size_t)(k0 + ac) * L.CS + nt * 8 + ar];
+                dmma884(acc[q][0], acc[q][1], a, b);
+              }
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < NTW; ++q) {
+        const int tile = warp + q * kLocMmaWarps;
+        if (tile >= MT * (kLocMmaCols / 8)) continue;
+        const int mt = tile / (kLocMmaCols / 8), nt = tile - mt * (kLocMmaCols / 8);
+        const int ii = i0 + mt * 8 + ar;
+        const int tt = nt * 8 + 2 * ac;
+        if (ii >= it.ni) continue;
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          if (tt + h < ncol) atomicAdd(&gs[(size_t)(cb + tt + h) * ld_gs + it.i0 + ii], sgn * acc[q][h]);
+      }
+    }
+  }
+}
+
+}  // namespace hankel

@@ -23,8 +23,12 @@ namespace hankel {
 // out[12] asymptotic boxes oversampled below sigma = 2
 // out[13] 1 if the asymptotic boxes run in FP32 (mixed precision), else 0
 // out[14] modelled worst-case error of the asymptotic boxes in FP32, per unit ||c||_1
+// out[15] planning ms: grid validation and box partition
+// out[16] planning ms: work lists
+// out[17] planning ms: device tables and uploads
+// out[18] 1 when the box partition ran on the device
 void plan_stats(const DevicePlan& D, double* out, int n) {
-  double s[15] = {0};
+  double s[19] = {0};
   for (const AsyBoxD& b : D.asyb) {
     double nj = b.j1 - b.j0 + 1, ni = b.i1 - b.i0 + 1;
     const AsyClass& K = D.classes[b.cls];
@@ -47,7 +51,11 @@ void plan_stats(const DevicePlan& D, double* out, int n) {
   s[11] = D.KL1;
   s[13] = D.mixed_asy ? 1.0 : 0.0;
   s[14] = D.fp32_err;
-  for (int i = 0; i < n && i < 15; ++i) out[i] = s[i];
+  s[15] = D.plan_ms[0];
+  s[16] = D.plan_ms[1];
+  s[17] = D.plan_ms[2];
+  s[18] = D.partition_on_device;
+  for (int i = 0; i < n && i < 19; ++i) out[i] = s[i];
 }
 
 namespace {

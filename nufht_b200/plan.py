@@ -57,9 +57,10 @@ class DevicePlan:
         self.mixed = mixed
 
     def stats(self):
-        """Work counts of the plan and its FP32 error model (nufht_b200_plan_stats, 15 values)."""
-        st = np.zeros(15)
-        L.lib().nufht_b200_plan_stats(self._h, st.ctypes.data_as(L.c_double_p), 15)
+        """Work counts of the plan, its FP32 error model and its planning time
+        (nufht_b200_plan_stats, 19 values)."""
+        st = np.zeros(19)
+        L.lib().nufht_b200_plan_stats(self._h, st.ctypes.data_as(L.c_double_p), 19)
         return st
 
     def info(self):

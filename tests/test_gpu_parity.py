@@ -312,6 +312,33 @@ def test_direct_box_large_against_oracle(cuda, orc, nu, shape):
     assert col_err(g, gd, c).max() <= 1e-12, (nu, shape)
 
 
+@pytest.mark.parametrize("nu,B,K,ni", [(0.0, 1, None, 1200), (3.0, 70, None, 333), (10.0, 5, None, 129),
+                                        (100.0, 9, 200, 300), (-7.0, 33, None, 17)])
+def test_local_box_tensor_core_contractions(cuda, orc, nu, B, K, ni):
+    """add_loc_batch on the FP64 tensor-core kernels (Chebyshev projection and Bessel-product
+    evaluation as DMMA tiles): Wimp degrees from the tables and a degree of 200 at order 100
+    (Bessel tables of 251 orders per target), one column, more than one 64-column pass, target
+    counts that are not multiples of the tile, against the oracle's direct sums."""
+    from nufht_b200 import _lib as L
+    lib = L.lib()
+    rng = np.random.default_rng(int(abs(nu)) + B)
+    rc, z, ka, kl, coef = orc.plan_params(abs(nu), 1e-8)
+    if K is None:
+        K = kl
+        r = np.sort(rng.uniform(0.1, 3, 2500))
+        k = np.sort(rng.uniform(0.01, 0.95 * z / 3.0, ni))
+    else:
+        r = np.sort(rng.uniform(0.5, 50.0, 2500))
+        k = np.sort(rng.uniform(0.01, 2.0, ni))
+    m, n = len(r), len(k)
+    c = np.asfortranarray(rng.standard_normal((m, B)))
+    g0 = np.asfortranarray(rng.standard_normal((n, B)))
+    g = g0.copy(order="F")
+    lib.add_loc_batch(L.dptr(g), nu, L.dptr(r), L.dptr(c), L.dptr(k), m, n, K, B, m, n, None, None, None)
+    gd = orc.direct_sum(abs(nu), r, k, c, np.arange(n))
+    assert col_err(g - g0, gd, c).max() <= 1e-8, (nu, B, K)
+
+
 def test_launch_counter_moves(cuda):
     from nufht_b200 import _lib as L
     from nufht_b200 import _pynufht as pn
