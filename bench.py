@@ -217,6 +217,112 @@ def cpu_baseline_leg(N, M, B, runs):
                               "runs_s": t_one}}
 
 
+def batch_problems(rng, count, nmax=100_000):
+    """The batching workload: `count` independent transforms with nu in {0, 1/2, 1, 2, 7/2, 10},
+    N and M log-uniform integers in [1e3, nmax], r and k uniform on (0, R] and (0, K] with R, K
+    log-uniform in [10, 1e3], 1-16 columns of N(0,1), tol in {1e-4, 1e-8, 1e-12}."""
+    out = []
+    for _ in range(count):
+        nu = float(rng.choice([0.0, 0.5, 1.0, 2.0, 3.5, 10.0]))
+        N = int(10.0 ** rng.uniform(3, np.log10(nmax)))
+        M = int(10.0 ** rng.uniform(3, np.log10(nmax)))
+        R = 10.0 ** rng.uniform(1, 3)
+        K = 10.0 ** rng.uniform(1, 3)
+        r = np.sort(R * (1.0 - rng.random(N)))
+        k = np.sort(K * (1.0 - rng.random(M)))
+        B = int(rng.integers(1, 17))
+        tol = float(rng.choice([1e-4, 1e-8, 1e-12]))
+        out.append((nu, r, k, B, tol, rng.standard_normal((B, N))))
+    return out
+
+
+def batch_figure(dev, st, steps):
+    """256 independent transforms (the batching workload) in one CUDA-graph launch, against the
+    same plans launched one after another on one stream: Gpts*cols/s = sum (N + M) B / t for one
+    (forward) transform of every problem, device time with CUDA events."""
+    import torch
+    from nufht_b200 import DevicePlan
+    from nufht_b200.batch import TransformBatch
+    probs = batch_problems(np.random.default_rng(4), 256)
+    t0 = time.perf_counter()
+    plans = [DevicePlan(nu, r, k, tol) for nu, r, k, B, tol, c in probs]
+    plan_s = time.perf_counter() - t0
+    items = [(p, torch.tensor(c, device=dev)) for p, (nu, r, k, B, tol, c) in zip(plans, probs)]
+    outs = [torch.empty((c.shape[0], p.n), dtype=torch.float64, device=dev) for p, c in items]
+    t0 = time.perf_counter()
+    tb = TransformBatch(items)
+    create_s = time.perf_counter() - t0
+    work = float(sum((len(r) + len(k)) * B for nu, r, k, B, tol, c in probs))
+
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    def sequential():
+        for (p, c), o in zip(items, outs):
+            p.execute_columns(c, o, st)
+
+    ms_graph = timed(lambda: tb.launch(st), steps)
+    ms_seq = timed(sequential, max(1, steps // 2))
+    info = tb.info()
+    tb.close()
+    for p in plans:
+        p.close()
+    return {"workload": "256 transforms: nu in {0,1/2,1,2,7/2,10}, N,M log-uniform in [1e3,1e5], "
+                        "R,K log-uniform in [10,1e3], 1-16 columns, tol in {1e-4,1e-8,1e-12}; one forward each",
+            "unit": UNIT, "value": work / (ms_graph * 1e-3) / 1e9, "ms": ms_graph,
+            "sequential": {"value": work / (ms_seq * 1e-3) / 1e9, "ms": ms_seq},
+            "graph_over_sequential": ms_seq / ms_graph, "branches": info["branches"],
+            "kernel_nodes": info["kernel_nodes"], "planning_s": plan_s, "batch_create_s": create_s}
+
+
+def planning_figure(dev):
+    """Planning cost (host wall-clock, device-side box partition) of this workload's forward
+    plan (1e6 x 1e6, nu = 0, tol 1e-8) and of the 4e6 x 4e6 order-100 stress grids, beside
+    the first and a later transform of 32 columns."""
+    import torch
+    from nufht_b200 import DevicePlan
+    out = {}
+    rng = np.random.default_rng(1)
+    r = np.sort(1000.0 * (1.0 - rng.random(1_000_000)))
+    k = np.sort(1000.0 * (1.0 - rng.random(1_000_000)))
+    rng = np.random.default_rng(100)
+    n = 4_000_000
+    means = np.array([200.0, 800.0, 1500.0])
+    rr = np.sort(np.clip(np.abs(rng.normal(means[rng.integers(0, 3, n)], 50.0)), 1e-9, 2000.0))
+    kk = np.sort(2000.0 * (1.0 - rng.random(n)))
+    for name, a, b, nu, kw in (("1e6_nu0", r, k, 0.0, {}), ("4e6_nu100", rr, kk, 100.0, {"extended_tables": True})):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        p = DevicePlan(nu, a, b, 1e-8, mixed="averaged", **kw)
+        torch.cuda.synchronize(dev)
+        create_ms = (time.perf_counter() - t0) * 1e3
+        st = p.stats()
+        c = torch.randn((32, len(a)), dtype=torch.float64, device=dev)
+        times = []
+        for _ in range(3):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            p.execute_columns(c)
+            torch.cuda.synchronize(dev)
+            times.append((time.perf_counter() - t0) * 1e3)
+        out[name] = {"plan_create_ms": create_ms, "partition_ms": st[15], "work_lists_ms": st[16],
+                     "tables_upload_ms": st[17], "partition_on_device": bool(st[18]),
+                     "first_transform_ms": times[0], "transform_ms": min(times[1:])}
+        p.close()
+        del c
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -227,6 +333,7 @@ def main():
     ap.add_argument("--n", type=int, default=1000000)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the batching and planning figures")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     N = M = args.n
@@ -449,6 +556,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_leg(N, M, B, 3)
 
+    extra = None
+    if rank == 0 and world == 1 and not args.no_extra:
+        extra = {"batch_256": batch_figure(dev, st, args.steps), "planning": planning_figure(dev)}
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
@@ -456,7 +567,7 @@ def main():
                 "data": "synthetic (seeded numpy draws with the workload's shapes)", "config": config,
                 "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches),
                 "phases_ms_per_step": phases, "roofline": roofline, "cpu_baseline": cpu,
-                "fp64_form": fp64, "accuracy": accuracy, "plan": pf.info()}
+                "fp64_form": fp64, "accuracy": accuracy, "plan": pf.info(), "extra": extra}
         print(json.dumps(line))
     pf.close()
     pa.close()

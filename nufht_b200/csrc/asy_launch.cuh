@@ -13,14 +13,14 @@
 namespace hankel {
 namespace {
 
-AsyShape asy_shape(const DevicePlan& D, int B, int LPT) {
+AsyShape asy_shape(int NLP, int B, int LPT) {
   AsyShape L;
   L.LPT = LPT;
-  L.NG = D.NLP / LPT;
+  L.NG = NLP / LPT;
   int cap = std::max(1, std::min(256 / L.NG, 32));
   L.BT = std::min(cap, B);
   L.threads = L.BT * L.NG;
-  L.V_total = D.NLP * B;
+  L.V_total = NLP * B;
   L.ngy = (B + L.BT - 1) / L.BT;
   return L;
 }
@@ -29,8 +29,8 @@ template <typename T, int W, int LPT, bool WINDOWED>
 int launch_spread_kind(DevicePlan& D, const AsyClass& K, int item0, int nitems, const double* cs, int ld_cs,
                        int B, cudaStream_t st) {
   if (nitems == 0) return 0;
-  const AsyShape L = asy_shape(D, B, LPT);
-  size_t sm = spread_smem<T>(W, L.BT * D.NLP, L.NG, L.BT, WINDOWED).total;
+  const AsyShape L = asy_shape(K.ac.NLP, B, LPT);
+  size_t sm = spread_smem<T>(W, L.BT * K.ac.NLP, L.NG, L.BT, WINDOWED, spread_tile_cells(K.ac.NLP)).total;
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(k_asy_spread<T, W, LPT, WINDOWED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -55,8 +55,8 @@ int launch_spread_lpt(DevicePlan& D, const AsyClass& K, const double* cs, int ld
 template <typename T, int W, int LPT>
 int launch_interp_lpt(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, int B, cudaStream_t st,
                       double sgn) {
-  const AsyShape L = asy_shape(D, B, LPT);
-  size_t sm = interp_smem<T>(W, D.NLP, L.threads).total;
+  const AsyShape L = asy_shape(K.ac.NLP, B, LPT);
+  size_t sm = interp_smem<T>(W, K.ac.NLP, L.threads).total;
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(k_asy_interp<T, W, LPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
@@ -71,10 +71,12 @@ int launch_interp_lpt(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, i
 }
 
 // Terms per thread (register blocking): LPT = 2, or 1 in double precision for windows wider
-// than 10 (register budget); NLP = 2 (K + 1) is even.
+// than 10 (register budget) and for classes of at most 4 terms (so that a CTA keeps at least
+// two warps' worth of threads, NLP / LPT per column); NLP = 2 (K + 1) is even.
 template <typename T, int W>
 int launch_spread(DevicePlan& D, const AsyClass& K, const double* cs, int ld_cs, int B, cudaStream_t st) {
   if constexpr (sizeof(T) == 8 && W > 10) return launch_spread_lpt<T, W, 1>(D, K, cs, ld_cs, B, st);
+  else if (K.ac.NLP <= 4) return launch_spread_lpt<T, W, 1>(D, K, cs, ld_cs, B, st);
   else return launch_spread_lpt<T, W, 2>(D, K, cs, ld_cs, B, st);
 }
 
@@ -83,6 +85,7 @@ template <typename T, int W>
 int launch_interp(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, int B, cudaStream_t st, double sgn) {
   if (K.ninterp == 0) return 0;
   if constexpr (sizeof(T) == 8 && W > 10) return launch_interp_lpt<T, W, 1>(D, K, gs, ld_gs, B, st, sgn);
+  else if (K.ac.NLP <= 4) return launch_interp_lpt<T, W, 1>(D, K, gs, ld_gs, B, st, sgn);
   else return launch_interp_lpt<T, W, 2>(D, K, gs, ld_gs, B, st, sgn);
 }
 
@@ -110,24 +113,37 @@ int run_asy_t(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs,
               double sgn) {
   using C2 = typename Cplx<T>::type;
   int rc = 0;
-  const size_t V = (size_t)D.NLP * B;
   C2* grid = static_cast<C2*>(D.d_grid);
   {
     PhaseScope ps(kPhaseSpread, st);
     if (D.chunk_cell_end > D.chunk_cell_begin)
-      NUFHT_CUDA_TRY(cudaMemsetAsync(grid + (size_t)D.chunk_cell_begin * V, 0,
-                                     sizeof(C2) * (size_t)(D.chunk_cell_end - D.chunk_cell_begin) * V, st));
+      NUFHT_CUDA_TRY(cudaMemsetAsync(grid + (size_t)D.chunk_cell_begin * B, 0,
+                                     sizeof(C2) * (size_t)(D.chunk_cell_end - D.chunk_cell_begin) * B, st));
+    // the classes' boxes own disjoint grid ranges: their launches run concurrently
+    int used[DevicePlan::kAuxStreams];
+    int nu = 0;
     for (const AsyClass& K : D.classes) {
       if (K.nspread + K.nspreadA == 0) continue;
-      NUFHT_W_DISPATCH(launch_spread, T, K.W, D, K, cs, ld_cs, B, st);
+      if (nu < DevicePlan::kAuxStreams - 2) {
+        used[nu] = 2 + nu;
+        ++nu;
+      }
+    }
+    if ((rc = fork_streams(D, st, used, nu))) return rc;
+    int q = 0;
+    for (const AsyClass& K : D.classes) {
+      if (K.nspread + K.nspreadA == 0) continue;
+      cudaStream_t cs_st = D.serial ? st : D.aux[used[q++ % nu]];
+      NUFHT_W_DISPATCH(launch_spread, T, K.W, D, K, cs, ld_cs, B, cs_st);
       if (rc) return rc;
     }
+    if ((rc = join_streams(D, st, used, nu))) return rc;
   }
   {
     PhaseScope ps(kPhaseFft, st);
     for (const FftGroup& gr : D.groups) {
       cufftSetStream(gr.plan, st);
-      C2* p = grid + (size_t)gr.cell_off * V;
+      C2* p = grid + (size_t)gr.cell_off * B;
       cufftResult fr;
       if (sizeof(T) == 8)
         fr = cufftExecZ2Z(gr.plan, (cufftDoubleComplex*)p, (cufftDoubleComplex*)p, CUFFT_INVERSE);
@@ -138,11 +154,25 @@ int run_asy_t(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs,
   }
   {
     PhaseScope ps(kPhaseInterp, st);
+    // the classes add into g with atomics: their launches run concurrently
+    int used[DevicePlan::kAuxStreams];
+    int nu = 0;
     for (const AsyClass& K : D.classes) {
       if (K.ninterp == 0) continue;
-      NUFHT_W_DISPATCH(launch_interp, T, K.W, D, K, gs, ld_gs, B, st, sgn);
+      if (nu < DevicePlan::kAuxStreams - 2) {
+        used[nu] = 2 + nu;
+        ++nu;
+      }
+    }
+    if ((rc = fork_streams(D, st, used, nu))) return rc;
+    int q = 0;
+    for (const AsyClass& K : D.classes) {
+      if (K.ninterp == 0) continue;
+      cudaStream_t cs_st = D.serial ? st : D.aux[used[q++ % nu]];
+      NUFHT_W_DISPATCH(launch_interp, T, K.W, D, K, gs, ld_gs, B, cs_st, sgn);
       if (rc) return rc;
     }
+    if ((rc = join_streams(D, st, used, nu))) return rc;
   }
   return 0;
 }

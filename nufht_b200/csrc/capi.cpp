@@ -56,6 +56,18 @@ int host_copy(const double* p, int len, std::vector<double>* out) {
   return 0;
 }
 
+// Host view of a grid for planning: the caller's array itself when it is host memory, a copy
+// read back when it is device memory.
+int host_view(const double* p, int len, DevicePlan::HostGrid* out) {
+  if (!is_device_ptr(p)) {
+    out->borrow(p);
+    return 0;
+  }
+  int rc = host_copy(p, len, &out->own);
+  out->p = out->own.data();
+  return rc;
+}
+
 std::vector<HBox> to_hbox(const BoxVector& v) {
   std::vector<HBox> out;
   for (size_t q = 0; q < v.length; ++q) out.push_back({v.data[q].i0, v.data[q].i1, v.data[q].j0, v.data[q].j1});
@@ -150,6 +162,9 @@ int finish_device_plan(DevicePlan* D, int device) {
   const int rc = D->upload_all();
   D->plan_ms[1] = t1 - t0;
   D->plan_ms[2] = wall_ms() - t1;
+  // the host views may borrow the caller's arrays, which need not outlive planning
+  D->h_rs.release();
+  D->h_ws.release();
   return rc;
 }
 
@@ -167,8 +182,13 @@ int device_grids_and_boxes(DevicePlan* D, const double* rs, const double* ws, co
                            HBoxes* hb) {
   const int m = D->m, n = D->n;
   const double t0 = wall_ms();
+  static const bool report = [] {
+    const char* e = std::getenv("NUFHT_B200_PLAN_TIMING");
+    return e && e[0] == '1';
+  }();
   int rc;
-  if ((rc = host_copy(rs, m, &D->h_rs)) || (rc = host_copy(ws, n, &D->h_ws))) return rc;
+  if ((rc = host_view(rs, m, &D->h_rs)) || (rc = host_view(ws, n, &D->h_ws))) return rc;
+  const double t_copy = wall_ms();
   const int Kthr = D->P.K_loc < 0 ? 0 : D->P.K_loc;
   if (!use_device_planner()) {
     if (hankel::check_grid(D->h_rs.data(), m)) return NUFHT_E_UNSORTED_RS;
@@ -184,13 +204,17 @@ int device_grids_and_boxes(DevicePlan* D, const double* rs, const double* ws, co
   if (cudaMemcpy(D->d_rs, D->h_rs.data(), sizeof(double) * m, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(D->d_ws, D->h_ws.data(), sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
     return NUFHT_E_CUDA;
-  if ((rc = hankel::device_check_grid(D->d_rs, m, 0)) != 0) return rc == -1 ? NUFHT_E_UNSORTED_RS : rc;
-  if ((rc = hankel::device_check_grid(D->d_ws, n, 0)) != 0) return rc == -1 ? NUFHT_E_UNSORTED_WS : rc;
+  const double t_up = wall_ms();
+  int bad = 0;
   if ((rc = hankel::device_make_boxes(D->d_rs, m, D->d_ws, n, D->P.z_split, opt.max_levels, opt.min_dim_prod,
-                                      Kthr, hb, 0)))
+                                      Kthr, hb, 0, &bad)))
     return rc;
+  if (bad) return bad == 1 ? NUFHT_E_UNSORTED_RS : NUFHT_E_UNSORTED_WS;
   D->partition_on_device = 1;
   D->plan_ms[0] = wall_ms() - t0;
+  if (report)
+    std::fprintf(stderr, "nufht_b200 plan: host copies %.2f ms, upload %.2f ms, validation + partition %.2f ms\n",
+                 t_copy - t0, t_up - t_copy, wall_ms() - t_up);
   return 0;
 }
 
@@ -235,8 +259,18 @@ int device_state_for(const NufhtPlan* plan, DevicePlan** out) {
   D->P.nu = plan->nu; D->P.tol = plan->tol; D->P.z_split = plan->z_split;
   D->P.K_asy = plan->K_asy; D->P.K_loc = plan->K_loc;
   std::memcpy(D->P.asy_coef, plan->asy_coef, sizeof(plan->asy_coef));
+  {
+    // the table's switch points for fewer expansion terms at this order and tolerance
+    NufhtOptions o = nufht_default_options();
+    o.tol = plan->tol;
+    PlanParams Q;
+    if (hankel::fill_params(plan->nu, o, false, &Q) == 0) {
+      std::memcpy(D->P.z_terms, Q.z_terms, sizeof(Q.z_terms));
+      D->P.n_z_terms = std::min(Q.n_z_terms, plan->K_asy + 1);
+    }
+  }
   int rc;
-  if ((rc = host_copy(plan->rs, plan->m, &D->h_rs)) || (rc = host_copy(plan->ws, plan->n, &D->h_ws)))
+  if ((rc = host_view(plan->rs, plan->m, &D->h_rs)) || (rc = host_view(plan->ws, plan->n, &D->h_ws)))
     return rc;
   D->plan_loc = to_hbox(plan->boxes.loc);
   D->plan_asy = to_hbox(plan->boxes.asy);
@@ -445,7 +479,7 @@ void run_single_box(int kind, double* gs, double nu, const double* rs, const dou
     D->P.K_asy = K;
     if (asy_coef) std::memcpy(D->P.asy_coef, asy_coef, sizeof(double) * 64);
   }
-  if (host_copy(rs, m, &D->h_rs) || host_copy(ws, n, &D->h_ws)) {
+  if (host_view(rs, m, &D->h_rs) || host_view(ws, n, &D->h_ws)) {
     std::fprintf(stderr, "%s: cannot read grids\n", who);
     return;
   }
@@ -749,12 +783,11 @@ int nufht_b200_generate_boxes_device(const double* rs, int m, const double* ws, 
     dw = uw;
   }
   HBoxes hb;
-  rc = hankel::device_check_grid(dr, m, 0);
-  if (rc == 0) rc = hankel::device_check_grid(dw, n, 0) == 0 ? 0 : NUFHT_E_UNSORTED_WS;
-  else if (rc == -1) rc = NUFHT_E_UNSORTED_RS;
-  if (rc == 0) rc = hankel::device_make_boxes(dr, m, dw, n, z_split, max_levels, min_dim_prod, K_loc_threshold, &hb, 0);
+  int bad = 0;
+  rc = hankel::device_make_boxes(dr, m, dw, n, z_split, max_levels, min_dim_prod, K_loc_threshold, &hb, 0, &bad);
   release();
   if (rc) return rc;
+  if (bad) return bad == 1 ? NUFHT_E_UNSORTED_RS : NUFHT_E_UNSORTED_WS;
   out->loc = to_boxvec(hb.loc);
   out->asy = to_boxvec(hb.asy);
   out->dir = to_boxvec(hb.dir);
@@ -782,7 +815,7 @@ int nufht_b200_plan_info(const NufhtDevicePlan* plan, NufhtB200Info* info) {
   info->n_loc = (long)D->loc_boxes.size();
   info->n_asy = (long)D->asy_boxes.size();
   info->n_dir = (long)D->dir_boxes.size();
-  info->fft_points = D->total_cells;
+  info->fft_points = D->NLP > 0 ? D->total_cells / D->NLP : D->total_cells;
   info->spread_width = D->W;
   info->path = D->path;
   info->workspace_bytes = D->ws_bytes;

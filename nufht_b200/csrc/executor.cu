@@ -113,6 +113,16 @@ int next_pow2(int v) {
   return p;
 }
 
+// Expansion-term classes per oversampling class: NLP = 2, 4, ..., 2 kNlpClasses.
+constexpr int kNlpClasses = kMaxNLP / 2;
+
+// Asymptotic boxes split by expansion terms (NUFHT_B200_TERM_SPLIT=0 turns it off: every box
+// then takes the plan's 2 (K_asy + 1) terms, as the reference does).
+const bool term_split = [] {
+  const char* e = std::getenv("NUFHT_B200_TERM_SPLIT");
+  return !(e && e[0] == '0');
+}();
+
 // Oversampling factors tried for each asymptotic box.  sigma = 2 keeps the kernel
 // narrow (spreading-bound boxes with many points per cell); smaller sigma shrinks the
 // grid and the FFT (memory-bound boxes with few points per cell).
@@ -136,13 +146,15 @@ double fp32_error_bound(const DevicePlan& D, double kappa) {
   const double* rs = D.h_rs.data();
   const double* ws = D.h_ws.data();
   double err = 0.0;
-  for (const HBox& hb : D.asy_eval) {
+  for (size_t q = 0; q < D.asy_eval.size(); ++q) {
+    const HBox& hb = D.asy_eval[q];
+    const int nlp = q < D.asy_eval_nlp.size() ? D.asy_eval_nlp[q] : NLP;
     const double* p = std::upper_bound(rs + hb.j0, rs + hb.j1 + 1, 0.0);
     if (p > rs + hb.j1) continue;  // only sources at r = 0: nothing to evaluate
     const double x = ws[hb.i0] * *p;
     if (!(x > 0.0)) continue;
     double sum = 0.0;
-    for (int lp = 0; lp < NLP && lp < 64; ++lp) sum += s2p * std::fabs(D.P.asy_coef[lp]) * std::pow(x, -(lp + 0.5));
+    for (int lp = 0; lp < nlp && lp < 64; ++lp) sum += s2p * std::fabs(D.P.asy_coef[lp]) * std::pow(x, -(lp + 0.5));
     err = std::max(err, kFp32Err * kappa * sum);
   }
   return err;
@@ -203,6 +215,94 @@ AsyConst make_asy_const(const PlanParams& P, int NLP, int W, double beta) {
     A.qwpsi[q] = gw[q] * 0.25 * W * host_es(A.qx[q], W, beta);
   }
   return A;
+}
+
+// Expansion terms an asymptotic box needs: the smallest 2 (K + 1) whose table switch point
+// z_terms[K] is at most the box's smallest argument x_min = k_lo r_ref, never more than the
+// plan's 2 (K_asy + 1).
+int terms_needed(const PlanParams& P, int NLP, double xmin) {
+  for (int K = 0; K < P.n_z_terms && 2 * (K + 1) < NLP; ++K)
+    if (xmin >= P.z_terms[K]) return 2 * (K + 1);
+  return NLP;
+}
+
+// Split of the asymptotic boxes by expansion terms.  The reference evaluates every
+// asymptotic box with the K_asy + 1 term pairs that its smallest arguments (k r near z_split)
+// need; most of a large box lies at far larger k r, where fewer pairs meet the same
+// tolerance (the table's switch points for smaller K).  A box is cut along r at
+// r = z_terms[K] / k_lo or along k at k = z_terms[K] / r_ref when the modelled time of the two
+// parts (each with its own term count) is below the whole box's; the parts are split again
+// (greedily, a few levels).  Model per column, from B200 phase times at the 1e6-point
+// workload: spreading 71 ps per source and term, interpolation 99 ps per target and term,
+// FFT and grid traffic 288 ps per grid cell and term (sigma = 2).
+struct TermBox {
+  HBox b;
+  int nlp;
+};
+
+void split_by_terms(const PlanParams& P, int NLP, int W, const double* rs, const double* ws, const HBox& hb,
+                    int depth, std::vector<TermBox>* out) {
+  auto rref_of = [&](int j0, int j1) {
+    const double* p = std::upper_bound(rs + j0, rs + j1 + 1, 0.0);
+    return p <= rs + j1 ? *p : 0.0;
+  };
+  auto model = [&](const HBox& b, int* nlp_out) {
+    const double rref = rref_of(b.j0, b.j1);
+    const int nlp = rref > 0.0 ? terms_needed(P, NLP, ws[b.i0] * rref) : NLP;
+    if (nlp_out) *nlp_out = nlp;
+    const double X = 0.5 * (rs[b.j1] - rs[b.j0]);
+    const double S = std::max(0.5 * (ws[b.i1] - ws[b.i0]), 1e-12 * std::max(std::fabs(ws[b.i0]), 1.0));
+    const double half = std::ceil(X / (M_PI / (2.0 * S)) + 0.5 * W);
+    const double n2 = 2.0 * (2.0 * half + 1.0);
+    const double nj = b.j1 - b.j0 + 1, ni = b.i1 - b.i0 + 1;
+    return nlp * (71e-12 * nj + 99e-12 * ni + 288e-12 * n2);
+  };
+  int nlp0 = NLP;
+  const double c0 = model(hb, &nlp0);
+  if (P.n_z_terms == 0 || depth >= 6 || nlp0 <= 2) {
+    out->push_back({hb, nlp0});
+    return;
+  }
+  double best = c0;
+  HBox a{}, b{};
+  bool found = false;
+  const double rref = rref_of(hb.j0, hb.j1);
+  for (int K = 0; K < P.n_z_terms && 2 * (K + 1) < nlp0; ++K) {
+    const double zk = P.z_terms[K];
+    if (!std::isfinite(zk)) continue;
+    // along r: sources with r >= z_K / k_lo need at most K + 1 pairs
+    const int js = (int)(std::lower_bound(rs + hb.j0, rs + hb.j1 + 1, zk / ws[hb.i0]) - rs);
+    if (js > hb.j0 && js <= hb.j1) {
+      const HBox l{hb.i0, hb.i1, hb.j0, js - 1}, r{hb.i0, hb.i1, js, hb.j1};
+      const double c = model(l, nullptr) + model(r, nullptr);
+      if (c < best) {
+        best = c;
+        a = l;
+        b = r;
+        found = true;
+      }
+    }
+    // along k: targets with k >= z_K / r_ref
+    if (rref > 0.0) {
+      const int is = (int)(std::lower_bound(ws + hb.i0, ws + hb.i1 + 1, zk / rref) - ws);
+      if (is > hb.i0 && is <= hb.i1) {
+        const HBox l{hb.i0, is - 1, hb.j0, hb.j1}, r{is, hb.i1, hb.j0, hb.j1};
+        const double c = model(l, nullptr) + model(r, nullptr);
+        if (c < best) {
+          best = c;
+          a = l;
+          b = r;
+          found = true;
+        }
+      }
+    }
+  }
+  if (!found) {
+    out->push_back({hb, nlp0});
+    return;
+  }
+  split_by_terms(P, NLP, W, rs, ws, a, depth + 1, out);
+  split_by_terms(P, NLP, W, rs, ws, b, depth + 1, out);
 }
 
 }  // namespace
@@ -272,14 +372,31 @@ void DevicePlan::build_lists() {
   // interpolate (or spread) every point for all NLP x B vectors.
   dir.clear();
   asy_direct.clear();
+  asy_eval.clear();
+  asy_eval_nlp.clear();
+  W = spread_width(P.tol, 2.0);
+  NLP = 2 * (P.K_asy + 1);
   {
-    std::vector<HBox> kept;
+    std::vector<TermBox> parts;
     for (const HBox& hb : asy_boxes) {
       const int ni = hb.i1 - hb.i0 + 1, nj = hb.j1 - hb.j0 + 1;
-      if (std::min(ni, nj) <= kThinDirect) asy_direct.push_back(hb);
-      else kept.push_back(hb);
+      if (std::min(ni, nj) <= kThinDirect) {
+        asy_direct.push_back(hb);
+        continue;
+      }
+      parts.clear();
+      if (term_split) split_by_terms(P, NLP, W, rs, ws, hb, 0, &parts);
+      else parts.push_back({hb, NLP});
+      for (const TermBox& tb : parts) {
+        const int pi = tb.b.i1 - tb.b.i0 + 1, pj = tb.b.j1 - tb.b.j0 + 1;
+        if (std::min(pi, pj) <= kThinDirect) {
+          asy_direct.push_back(tb.b);
+        } else {
+          asy_eval.push_back(tb.b);
+          asy_eval_nlp.push_back(tb.nlp);
+        }
+      }
     }
-    asy_eval = kept;
   }
   std::vector<HBox> all_dir = dir_boxes;
   all_dir.insert(all_dir.end(), asy_direct.begin(), asy_direct.end());
@@ -300,8 +417,6 @@ void DevicePlan::build_lists() {
   interp.clear();
   groups.clear();
   classes.clear();
-  W = spread_width(P.tol, 2.0);
-  NLP = 2 * (P.K_asy + 1);
   int Wc[3];
   for (int c = 0; c < 3; ++c) Wc[c] = spread_width(P.tol, kSigmas[c]);
   // In FP32 the deconvolution by psi-hat amplifies rounding by psi-hat(0)/psi-hat(pi/sigma):
@@ -329,9 +444,11 @@ void DevicePlan::build_lists() {
     }
   }
   std::vector<AsyBoxD> tmp;
-  for (const HBox& hb : asy_eval) {
+  for (size_t q = 0; q < asy_eval.size(); ++q) {
+    const HBox& hb = asy_eval[q];
     AsyBoxD d;
     std::memset(&d, 0, sizeof(d));
+    d.nlp = asy_eval_nlp[q];
     d.i0 = hb.i0;
     d.i1 = hb.i1;
     d.j0 = hb.j0;
@@ -368,7 +485,7 @@ void DevicePlan::build_lists() {
     }
     const int Wb = Wc[best];
     const double sigma = kSigmas[best];
-    d.cls = best;
+    d.cls = best * kNlpClasses + std::min(d.nlp / 2 - 1, kNlpClasses - 1);  // class: (oversampling, terms)
     d.h = M_PI / (sigma * S);
     long long half = (long long)std::ceil(X / d.h + 0.5 * Wb);
     d.half = (int)half;
@@ -384,29 +501,34 @@ void DevicePlan::build_lists() {
       }
       return a;
     };
+    const int TC = spread_tile_cells(d.nlp);
     int worst = 0;
-    for (long long l = -half; l <= half; l += kSpreadTile)
-      worst = std::max(worst, first_ge(l + kSpreadTile + 1) - first_ge(l - Wb));
-    d.mode = worst > kTileMaxSources ? 1 : 0;
+    for (long long l = -half; l <= half; l += TC)
+      worst = std::max(worst, first_ge(l + TC + 1) - first_ge(l - Wb));
+    d.mode = (long long)worst * kSpreadTile > (long long)kTileMaxSources * TC ? 1 : 0;
     tmp.push_back(d);
   }
-  // Layout: groups of consecutive boxes with equal (mode, n2), mode-1 groups first so that
-  // their cells form one range to zero before spreading.
+  // Layout: groups of consecutive boxes with equal (mode, n2, terms), mode-1 groups first so
+  // that their cells form one range to zero before spreading.
   std::vector<int> order(tmp.size());
   for (size_t q = 0; q < order.size(); ++q) order[q] = (int)q;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
     if (tmp[a].mode != tmp[b].mode) return tmp[a].mode > tmp[b].mode;
+    if (tmp[a].nlp != tmp[b].nlp) return tmp[a].nlp > tmp[b].nlp;
     return tmp[a].n2 < tmp[b].n2;
   });
   long long row = 0, coff = 0, poff = 0;
   chunk_cell_begin = chunk_cell_end = 0;
   for (size_t q = 0; q < order.size();) {
     size_t e = q;
-    while (e < order.size() && tmp[order[e]].n2 == tmp[order[q]].n2 && tmp[order[e]].mode == tmp[order[q]].mode) ++e;
+    while (e < order.size() && tmp[order[e]].n2 == tmp[order[q]].n2 && tmp[order[e]].mode == tmp[order[q]].mode &&
+           tmp[order[e]].nlp == tmp[order[q]].nlp)
+      ++e;
     FftGroup gr;
     gr.n2 = tmp[order[q]].n2;
     gr.nbox = (int)(e - q);
     gr.mode = tmp[order[q]].mode;
+    gr.nlp = tmp[order[q]].nlp;
     gr.cell_off = row;
     gr.plan = 0;
     for (size_t z = q; z < e; ++z) {
@@ -416,7 +538,7 @@ void DevicePlan::build_lists() {
       d.post_off = poff;
       coff += 2LL * d.half + 1;
       poff += d.i1 - d.i0 + 1;
-      row += d.n2;
+      row += (long long)d.n2 * d.nlp;
       asyb.push_back(d);
     }
     if (gr.mode == 1) chunk_cell_end = row;
@@ -429,13 +551,27 @@ void DevicePlan::build_lists() {
   // Work items, grouped by kernel class: windowed spreading items (mode 0 tiles and mode 2
   // zero padding), then atomic ones (mode 1 chunks of dense boxes).
   std::vector<SpreadItem> atomic_items;
-  for (int c = 0; c < 3; ++c) {
+  for (int c = 0; c < 3 * kNlpClasses; ++c) {
     AsyClass K;
-    K.sigma = kSigmas[c];
-    K.W = Wc[c];
+    K.sigma = kSigmas[c / kNlpClasses];
+    K.W = Wc[c / kNlpClasses];
+    K.nlp = 2 * (c % kNlpClasses + 1);
     K.spread0 = (int)spread.size();
     K.interp0 = (int)interp.size();
     bool any = false;
+    // Sources per dense-box chunk: at most kChunkSources, fewer when the class's dense boxes
+    // would otherwise give less than about four CTAs per SM (a chunk is one CTA walking its
+    // sources in order).
+    int chunk_src = kChunkSources;
+    {
+      long long dense = 0;
+      for (const AsyBoxD& d : asyb)
+        if (d.cls == c && d.mode == 1) dense += d.j1 - d.j0 + 1;
+      if (dense > 0) {
+        const long long want = dense / (148LL * 4LL);
+        chunk_src = (int)std::min<long long>(kChunkSources, std::max<long long>(256, (want + 63) / 64 * 64));
+      }
+    }
     for (size_t b = 0; b < asyb.size(); ++b) {
       const AsyBoxD& d = asyb[b];
       if (d.cls != c) continue;
@@ -464,24 +600,25 @@ void DevicePlan::build_lists() {
           s.je = first_ge((long long)l_start + ncell);
           spread.push_back(s);
         };
-        for (int l = 0; l <= d.half; l += kSpreadTile) add_tile(l, std::min(kSpreadTile, d.half - l + 1), l);
-        for (int l = -1; l >= -d.half; l -= kSpreadTile) {
-          int lo = std::max(l - kSpreadTile + 1, -d.half);
+        const int TC = spread_tile_cells(d.nlp);
+        for (int l = 0; l <= d.half; l += TC) add_tile(l, std::min(TC, d.half - l + 1), l);
+        for (int l = -1; l >= -d.half; l -= TC) {
+          int lo = std::max(l - TC + 1, -d.half);
           add_tile(lo, l - lo + 1, d.n2 + lo);
         }
-        for (int f = d.half + 1; f <= d.n2 - d.half - 1; f += 4 * kSpreadTile) {
+        for (int f = d.half + 1; f <= d.n2 - d.half - 1; f += 4 * TC) {
           SpreadItem s;
           s.box = (int)b;
           s.mode = 2;
           s.l_start = 0;
           s.fft_start = f;
-          s.ncell = std::min(4 * kSpreadTile, d.n2 - d.half - f);
+          s.ncell = std::min(4 * TC, d.n2 - d.half - f);
           s.js = s.je = 0;
           spread.push_back(s);
         }
       } else {
-        // Dense box: chunks of kChunkSources sources, added atomically to the grid.
-        for (int js = d.j0; js <= d.j1; js += kChunkSources) {
+        // Dense box: chunks of chunk_src sources, added atomically to the grid.
+        for (int js = d.j0; js <= d.j1; js += chunk_src) {
           SpreadItem s;
           s.box = (int)b;
           s.mode = 1;
@@ -489,7 +626,7 @@ void DevicePlan::build_lists() {
           s.ncell = 0;
           s.fft_start = 0;
           s.js = js;
-          s.je = std::min(js + kChunkSources, d.j1 + 1);
+          s.je = std::min(js + chunk_src, d.j1 + 1);
           atomic_items.push_back(s);
         }
       }
@@ -502,7 +639,7 @@ void DevicePlan::build_lists() {
     K.nspreadA = (int)atomic_items.size();
     atomic_items.clear();
     K.ninterp = (int)interp.size() - K.interp0;
-    if (any) K.ac = make_asy_const(P, NLP, K.W, es_beta(K.sigma, K.W));
+    if (any) K.ac = make_asy_const(P, K.nlp, K.W, es_beta(K.sigma, K.W));
     else std::memset(&K.ac, 0, sizeof(K.ac));
     classes.push_back(K);
   }
@@ -595,6 +732,11 @@ DevicePlan::~DevicePlan() {
   cudaFree(d_grid); cudaFree(d_partial); cudaFree(d_cheb); cudaFree(d_fft_work);
   for (void* p : retired) cudaFree(p);
   cudaFree(d_stage_c); cudaFree(d_stage_g); cudaFree(d_stage_t);
+  for (int q = 0; q < kAuxStreams; ++q) {
+    if (aux[q]) cudaStreamDestroy(aux[q]);
+    if (ev_join[q]) cudaEventDestroy(ev_join[q]);
+  }
+  if (ev_fork) cudaEventDestroy(ev_fork);
   if (copy_in) cudaStreamDestroy(copy_in);
   if (copy_out) cudaStreamDestroy(copy_out);
   for (int q = 0; q < 4; ++q) {
@@ -611,7 +753,6 @@ int DevicePlan::ensure_fft(int B) {
   if (asyb.empty() || B == fft_B) return 0;
   auto it = fft_cache.find(B);
   if (it == fft_cache.end()) {
-    const long long V = (long long)NLP * B;
     size_t need = 0;
     std::vector<cufftHandle> hs;
     auto destroy = [&]() {
@@ -626,7 +767,7 @@ int DevicePlan::ensure_fft(int B) {
       hs.push_back(h);
       cufftSetAutoAllocation(h, 0);
       int nn = gr.n2;
-      long long batch = (long long)gr.nbox * V;
+      long long batch = (long long)gr.nbox * gr.nlp * B;
       if (batch > INT_MAX) {
         destroy();
         return NUFHT_E_TOO_LARGE;
@@ -661,15 +802,42 @@ int DevicePlan::ensure_fft(int B) {
   return 0;
 }
 
+int DevicePlan::ensure_aux() {
+  if (ev_fork) return 0;
+  for (int q = 0; q < kAuxStreams; ++q) {
+    NUFHT_CUDA_TRY(cudaStreamCreateWithFlags(&aux[q], cudaStreamNonBlocking));
+    NUFHT_CUDA_TRY(cudaEventCreateWithFlags(&ev_join[q], cudaEventDisableTiming));
+  }
+  NUFHT_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+  return 0;
+}
+
+// Fork: streams s[0..n) wait for the work queued so far on st.  Join: st waits for all of
+// them.  Both are ordinary event records and waits, so they are captured into CUDA graphs as
+// dependencies.
+int fork_streams(DevicePlan& D, cudaStream_t st, const int* which, int n) {
+  if (D.serial) return 0;
+  NUFHT_CUDA_TRY(cudaEventRecord(D.ev_fork, st));
+  for (int q = 0; q < n; ++q) NUFHT_CUDA_TRY(cudaStreamWaitEvent(D.aux[which[q]], D.ev_fork, 0));
+  return 0;
+}
+int join_streams(DevicePlan& D, cudaStream_t st, const int* which, int n) {
+  if (D.serial) return 0;
+  for (int q = 0; q < n; ++q) {
+    NUFHT_CUDA_TRY(cudaEventRecord(D.ev_join[which[q]], D.aux[which[q]]));
+    NUFHT_CUDA_TRY(cudaStreamWaitEvent(st, D.ev_join[which[q]], 0));
+  }
+  return 0;
+}
+
 int DevicePlan::ensure_workspace(int B) {
   if (B <= ws_B) return ensure_fft(B);
   drop_buffer(d_grid); drop_buffer(d_partial); drop_buffer(d_cheb);
   d_grid = nullptr; d_partial = nullptr; d_cheb = nullptr;
   ws_B = 0;
   size_t bytes = 0;
-  const long long V = (long long)NLP * B;
   if (!asyb.empty()) {
-    size_t g = (size_t)total_cells * (size_t)V * (mixed_asy ? sizeof(float2) : sizeof(double2));
+    size_t g = (size_t)total_cells * (size_t)B * (mixed_asy ? sizeof(float2) : sizeof(double2));
     NUFHT_CUDA_TRY(cudaMalloc((void**)&d_grid, g));
     bytes += g;
   }
@@ -856,33 +1024,40 @@ int DevicePlan::run(const double* cs, int ld_cs, double* gs, int ld_gs, int B, c
   NUFHT_CUDA_TRY(cudaSetDevice(device));
   int rc = ensure_workspace(B);
   if (rc) return rc;
+  if ((rc = ensure_aux())) return rc;
+  // With per-phase timing on, everything runs in order on st (the phase times then add up to
+  // the transform's time; concurrent phases would overlap in time and share the GPU).
+  serial = g_phase_timing.load(std::memory_order_relaxed);
   if (zero_output) {
     PhaseScope ps(kPhaseZero, st);
     NUFHT_CUDA_TRY(cudaMemset2DAsync(gs, sizeof(double) * (size_t)ld_gs, 0, sizeof(double) * (size_t)n, B, st));
   }
   const double sgn = sign;
-  // ---- local boxes
+  // The three box families add into g with atomics and share no workspace, so the local and
+  // direct boxes run on their own streams beside the asymptotic ones (the FP64 Bessel work of
+  // the direct boxes overlaps the memory-bound FFT and grid passes).
+  const int side[2] = {0, 1};
+  if ((rc = fork_streams(*this, st, side, 2))) return rc;
+  const cudaStream_t s_loc = serial ? st : aux[0], s_dir = serial ? st : aux[1];
   if (!locb.empty()) {
     rc = launch_loc(d_rs, d_ws, cs, ld_cs, gs, ld_gs, B, d_locb, (int)locb.size(), d_proj, (int)proj.size(), d_eval,
-                    (int)eval.size(), d_partial, d_cheb, K_eval, nu2 / 2, sgn, st);
+                    (int)eval.size(), d_partial, d_cheb, K_eval, nu2 / 2, sgn, s_loc);
     if (rc) return rc;
   }
-  // ---- asymptotic boxes
+  if (!dir.empty()) {
+    PhaseScope ps(kPhaseDir, s_dir);
+    if (B >= 32) rc = launch_dir<32>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);
+    else if (B >= 16) rc = launch_dir<16>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);
+    else if (B >= 8) rc = launch_dir<8>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);
+    else if (B >= 4) rc = launch_dir<4>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);
+    else rc = launch_dir<1>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);
+    if (rc) return rc;
+  }
   if (!asyb.empty()) {
     rc = run_asy(*this, cs, ld_cs, gs, ld_gs, B, st, sgn);
     if (rc) return rc;
   }
-  // ---- direct boxes
-  if (!dir.empty()) {
-    PhaseScope ps(kPhaseDir, st);
-    if (B >= 32) rc = launch_dir<32>(*this, cs, ld_cs, gs, ld_gs, B, st, sgn);
-    else if (B >= 16) rc = launch_dir<16>(*this, cs, ld_cs, gs, ld_gs, B, st, sgn);
-    else if (B >= 8) rc = launch_dir<8>(*this, cs, ld_cs, gs, ld_gs, B, st, sgn);
-    else if (B >= 4) rc = launch_dir<4>(*this, cs, ld_cs, gs, ld_gs, B, st, sgn);
-    else rc = launch_dir<1>(*this, cs, ld_cs, gs, ld_gs, B, st, sgn);
-    if (rc) return rc;
-  }
-  return 0;
+  return join_streams(*this, st, side, 2);
 }
 
 // The local-expansion kernels of one box on caller-provided device buffers (work lists,

@@ -39,7 +39,8 @@ struct AsyBoxD {
                         // <= z_split^-(lp+1/2), so both stay in single-precision range
   int half, n2;
   int mode;             // 0: CTAs own grid tiles; 1: CTAs own source chunks (dense boxes)
-  int cls;              // kernel class (oversampling and kernel width)
+  int cls;              // kernel class (oversampling, kernel width, expansion terms)
+  int nlp;              // expansion terms of this box: 2 (K + 1) with K <= K_asy
   long long cell_off;   // workspace offset in cells of one vector
   long long corr_off;   // first of 2 half + 1 entries in the cell table
   long long post_off;   // first of i1 - i0 + 1 entries in the target table
@@ -53,7 +54,7 @@ struct SpreadItem {
 };
 struct InterpItem { int box, ks, ke; };
 struct FftGroup {
-  int n2, nbox, mode;
+  int n2, nbox, mode, nlp;
   long long cell_off;  // the group's boxes are consecutive in the workspace
   cufftHandle plan;
 };
@@ -69,10 +70,12 @@ struct AsyConst {
 };
 
 // A kernel class: oversampling factor sigma of both type-3 stages, kernel width W and
-// shape beta, and the contiguous ranges of its boxes' spreading / interpolation items.
+// shape beta, expansion terms NLP (ac.NLP), and the contiguous ranges of its boxes'
+// spreading / interpolation items.
 struct AsyClass {
   double sigma;
   int W;
+  int nlp;
   AsyConst ac;
   int spread0, nspread;    // windowed spreading items (modes 0 and 2)
   int spreadA0, nspreadA;  // atomic spreading items (mode 1)
@@ -90,10 +93,27 @@ struct DevicePlan {
   int path = 0;   // 0 boxes, 1 all-direct, 2 all-asymptotic
   int nu2 = 0;    // 2 |nu|
   double sign = 1.0;
-  std::vector<double> h_rs, h_ws;
+  // Host view of the grids, used while planning only: the caller's own array when the grid
+  // is in host memory (no copy), else a copy read back from the device.
+  struct HostGrid {
+    std::vector<double> own;
+    const double* p = nullptr;
+    const double* data() const { return p; }
+    double operator[](size_t i) const { return p[i]; }
+    void borrow(const double* q) {
+      own.clear();
+      p = q;
+    }
+    void release() {
+      std::vector<double>().swap(own);
+      p = nullptr;
+    }
+  };
+  HostGrid h_rs, h_ws;
   std::vector<HBox> loc_boxes, asy_boxes, dir_boxes;  // boxes as evaluated
   std::vector<HBox> plan_loc, plan_asy, plan_dir;     // the planner's partition
   std::vector<HBox> asy_eval, asy_direct;  // asymptotic boxes evaluated by NUFFT / summed directly
+  std::vector<int> asy_eval_nlp;            // expansion terms of each asy_eval box
 
   // work lists
   int KL1 = 0, W = 0;
@@ -107,7 +127,7 @@ struct DevicePlan {
   std::vector<InterpItem> interp;
   std::vector<FftGroup> groups;
   std::vector<AsyClass> classes;
-  long long total_cells = 0;       // grid rows: sum of n2 over asymptotic boxes
+  long long total_cells = 0;       // grid values per column: sum of n2 * NLP over asymptotic boxes
   long long chunk_cell_begin = 0;  // grid rows of the mode-1 boxes (zeroed before spreading)
   long long chunk_cell_end = 0;
   long long total_corr = 0, total_post = 0;
@@ -151,6 +171,15 @@ struct DevicePlan {
   double* d_stage_g = nullptr;
   double* d_stage_t = nullptr;  // row-major copies of cs / gs (nufht_b200_batch_layout)
   size_t stage_c_bytes = 0, stage_g_bytes = 0, stage_t_bytes = 0;
+  // Streams on which run() executes independent phases and kernel classes concurrently
+  // (forked from and joined back to the caller's stream with events; created on first use):
+  // 0 local boxes, 1 direct boxes, 2.. asymptotic kernel classes.
+  static constexpr int kAuxStreams = 8;
+  cudaStream_t aux[kAuxStreams] = {};
+  cudaEvent_t ev_fork = nullptr;
+  cudaEvent_t ev_join[kAuxStreams] = {};
+  int ensure_aux();
+  bool serial = false;  // this run() queues everything on the caller's stream
   // copy streams and events of the pipelined host-buffer path (created on first use)
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   cudaEvent_t ev_in[4] = {}, ev_done[4] = {};
@@ -212,11 +241,18 @@ int run_asy_f64(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_g
 
 int run_besselj(double nu, const double* x, double* out, long count, cudaStream_t st);
 
+// Fork streams D.aux[which[0..n)] from st (they wait for st's work so far) and join them back
+// (st waits for their work), with events.
+int fork_streams(DevicePlan& D, cudaStream_t st, const int* which, int n);
+int join_streams(DevicePlan& D, cudaStream_t st, const int* which, int n);
+
 // Device planner (planner_dev.cu): validation of a device-resident grid (0, or -1 when not
 // finite, non-negative and non-decreasing) and the box partition from device-resident grids.
 int device_check_grid(const double* d_a, int len, cudaStream_t st);
+// bad_grid (optional): also validate both grids; set to 0, or 1 / 2 when rs / ws is not
+// finite, non-negative and non-decreasing (the boxes are then not computed).
 int device_make_boxes(const double* d_rs, int m, const double* d_ws, int n, double z, int max_levels,
-                      int min_dim_prod, int Kthr, HBoxes* out, cudaStream_t st);
+                      int min_dim_prod, int Kthr, HBoxes* out, cudaStream_t st, int* bad_grid = nullptr);
 
 // out[c * ldo + r] = in[r * ldi + c] for r < rows, c < cols (device pointers): a row-major
 // batch to the executor's column-major one and back.

@@ -17,8 +17,9 @@
 // (mixed precision).  Cell indices, source and target phases, the deconvolution tables and
 // the final combination into g stay in FP64 in both.
 //
-// Workspace layout: box b owns n2 * V contiguous complex values, vector v = t * NLP + lp
-// at offset cell_off * V + v * n2 (one contiguous FFT input per vector).
+// Workspace layout: box b (with NLP expansion terms) owns n2 * NLP * B contiguous complex
+// values from cell_off * B (cell_off = the sum of n2 * NLP over the boxes before it); vector
+// v = t * NLP + lp starts at v * n2 within them (one contiguous FFT input per vector).
 #pragma once
 
 #include <climits>
@@ -27,14 +28,13 @@
 
 namespace hankel {
 
-constexpr int kSpreadTile = 16;     // cells owned by one mode-0 spreading CTA
+constexpr int kSpreadTile = 16;     // cells owned by one mode-0 spreading CTA at 8 or more terms
 constexpr int kMinFft = 32;         // smallest FFT length of a box
 constexpr int kSpreadChunk = 64;    // sources staged in shared memory per round
 constexpr int kChunkSources = 2048; // sources per mode-1 work item, at most
 constexpr int kTileMaxSources = 4096;
 constexpr int kInterpTile = 128;    // targets per interpolation CTA
 constexpr int kInterpChunk = 32;    // targets per shared-memory round
-constexpr int kInterpPrefetch = 8;  // cells between the L1 prefetch of a grid row and its fetch
 
 template <typename T> struct Cplx;
 template <> struct Cplx<double> { using type = double2; };
@@ -65,6 +65,12 @@ struct AsyShape {
   int LPT, NG, BT, threads, ngy, V_total;
 };
 
+// Cells of a mode-0 spreading tile: 16 at 6 or more expansion terms, 32 at 2 or 4 (whose
+// CTAs have one term per thread, NLP / 1 threads per column).  The shared window of a tile
+// (cells x (vectors + 1) complex values) decides how many CTAs fit on an SM: these sizes keep
+// it near 16 KB for 2 and 4 terms and 33 KB for 8, at least 16 warps per SM either way.
+__host__ __device__ constexpr int spread_tile_cells(int nlp) { return nlp >= 6 ? kSpreadTile : 2 * kSpreadTile; }
+
 // Staged kernel weights per source (complex) and per target (real), padded so that every
 // row is read with 16-byte shared-memory loads.
 template <typename T>
@@ -80,11 +86,11 @@ struct SpreadSmem {
   size_t win, wc, rq, c, u, ph, l0, end, total;
 };
 template <typename T>
-__host__ __device__ inline SpreadSmem spread_smem(int W, int VCTA, int NG, int BT, bool windowed) {
+__host__ __device__ inline SpreadSmem spread_smem(int W, int VCTA, int NG, int BT, bool windowed, int tile_cells) {
   SpreadSmem L{};
   const size_t c2 = 2 * sizeof(T);
   L.win = 0;
-  L.wc = align16(L.win + (windowed ? (size_t)kSpreadTile * (VCTA + 1) * c2 : 0));
+  L.wc = align16(L.win + (windowed ? (size_t)tile_cells * (VCTA + 1) * c2 : 0));
   L.rq = align16(L.wc + (size_t)kSpreadChunk * spread_we<T>(W) * c2);
   L.c = align16(L.rq + (size_t)kSpreadChunk * NG * c2);
   L.u = align16(L.c + (size_t)BT * (kSpreadChunk + 1) * sizeof(T));
@@ -237,7 +243,7 @@ __global__ void __launch_bounds__(256) k_asy_spread(
   const int nv = min(VCTA, V_total - v0);  // valid vectors of this CTA
   const int vloc = tl * NLP + g * LPT;     // first of this thread's vectors within the CTA
   const bool active = tl < BT && t0 + tl < B;
-  C2* gbox = grid + (size_t)bx.cell_off * (size_t)V_total;
+  C2* gbox = grid + (size_t)bx.cell_off * (size_t)B;
   const int nc = it.ncell;
 
   if (WINDOWED && it.mode == 2) {  // zero padding of the FFT input: threads along cells
@@ -249,8 +255,9 @@ __global__ void __launch_bounds__(256) k_asy_spread(
   }
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const SpreadSmem L = spread_smem<T>(W, VCTA, NG, BT, WINDOWED);
-  C2* win = reinterpret_cast<C2*>(smem_raw + L.win);        // [kSpreadTile][WP]
+  const int TC = spread_tile_cells(NLP);
+  const SpreadSmem L = spread_smem<T>(W, VCTA, NG, BT, WINDOWED, TC);
+  C2* win = reinterpret_cast<C2*>(smem_raw + L.win);        // [TC][WP]
   C2* s_wc = reinterpret_cast<C2*>(smem_raw + L.wc);        // [SCH][WE]
   C2* s_rq = reinterpret_cast<C2*>(smem_raw + L.rq);        // [SCH][NG]: (rho of term g LPT, rref / r)
   T* s_c = reinterpret_cast<T*>(smem_raw + L.c);            // [BT][SCP]
@@ -260,7 +267,7 @@ __global__ void __launch_bounds__(256) k_asy_spread(
   int* s_end = reinterpret_cast<int*>(smem_raw + L.end);    // [SCH]: end of the equal-l0 run
 
   if (WINDOWED)
-    for (int e = tid; e < kSpreadTile * WP; e += nthr) win[e] = cmake<T>(0, 0);
+    for (int e = tid; e < TC * WP; e += nthr) win[e] = cmake<T>(0, 0);
   const T ihw = (T)(2.0 / (double)W);
   const T beta = (T)P.beta;
 
@@ -440,7 +447,7 @@ __global__ void __launch_bounds__(256) k_asy_interp(
   const C2* row[LPT];
 #pragma unroll
   for (int u = 0; u < LPT; ++u)
-    row[u] = grid + (size_t)bx.cell_off * (size_t)V_total +
+    row[u] = grid + (size_t)bx.cell_off * (size_t)B +
              (size_t)(active ? (t0 + tl) * NLP + g * LPT + u : 0) * (size_t)n2;
   const T ihw = (T)(2.0 / (double)W);
   const T beta = (T)P.beta;
@@ -450,15 +457,7 @@ __global__ void __launch_bounds__(256) k_asy_interp(
     int idx = cell < 0 ? cell + n2 : (cell >= n2 ? cell - n2 : cell);
     return active ? row[u][idx] : cmake<T>(0, 0);
   };
-  // The ring fetches a cell one step before its stencil needs it, far less than a DRAM
-  // round trip; an L1 prefetch kInterpPrefetch cells further ahead (an address inside the
-  // row, wrapped like the fetch) makes those fetches L1 hits.
-  auto prefetch = [&](int cell, int u) {
-    if (!active) return;
-    int idx = cell % n2;
-    if (idx < 0) idx += n2;
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(row[u] + idx));
-  };
+
   // Stage targets [k0, k0 + nk) (all threads; barriers on both sides).
   auto stage = [&](int k0, int nk) {
     __syncthreads();
@@ -558,17 +557,12 @@ __global__ void __launch_bounds__(256) k_asy_interp(
       if (nxt == c + 1) {
         // the slot of cell c takes cell c + R (one cell ahead of the next stencil)
 #pragma unroll
-        for (int u = 0; u < LPT; ++u) {
-          gw[u][jj] = fetch(c + R, u);
-          prefetch(c + R + kInterpPrefetch, u);
-        }
+        for (int u = 0; u < LPT; ++u) gw[u][jj] = fetch(c + R, u);
       } else {
 #pragma unroll
         for (int q = 0; q < R; ++q)
 #pragma unroll
           for (int u = 0; u < LPT; ++u) gw[u][(jj + 1 + q) % R] = fetch(nxt + q, u);
-#pragma unroll
-        for (int u = 0; u < LPT; ++u) prefetch(nxt + R + kInterpPrefetch, u);
       }
       c = nxt;
     }

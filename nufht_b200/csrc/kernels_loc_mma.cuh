@@ -98,15 +98,17 @@ __global__ void __launch_bounds__(kLocThreads) k_loc_proj_mma(
     }
     __syncthreads();
     const int ar = lane >> 2, ac = lane & 3;
+    // sources outer, tiles inner: the warp's NT accumulator chains advance together
+    for (int k0 = 0; k0 < chunk; k0 += 4) {
+      const double* pa = sT + (size_t)ar * L.TS + k0 + ac;
+      const double* pb = sC + (size_t)(k0 + ac) * L.BS + ar;
 #pragma unroll
-    for (int q = 0; q < NT; ++q) {
-      const int tile = warp + q * kLocMmaWarps;
-      if (tile < ntiles) {
-        const int mt = tile / nnt, nt = tile - mt * nnt;
-        const double* pa = sT + (size_t)(mt * 8 + ar) * L.TS + ac;
-        const double* pb = sC + (size_t)ac * L.BS + nt * 8 + ar;
-#pragma unroll 4
-        for (int k0 = 0; k0 < chunk; k0 += 4) dmma884(acc[q][0], acc[q][1], pa[k0], pb[(size_t)k0 * L.BS]);
+      for (int q = 0; q < NT; ++q) {
+        const int tile = warp + q * kLocMmaWarps;
+        if (tile < ntiles) {
+          const int mt = tile / nnt, nt = tile - mt * nnt;
+          dmma884(acc[q][0], acc[q][1], pa[(size_t)mt * 8 * L.TS], pb[nt * 8]);
+        }
       }
     }
   }
@@ -143,13 +145,42 @@ inline LocEvalMma loc_eval_mma_layout(int TI, int maxo) {
   return L;
 }
 
+// Unnormalised J_0(z) .. J_nmax(z) into row[0..nmax] by Miller's downward recurrence (as
+// bessel_j_orders, bessel.cuh) and the factor 1/S that normalises them (S = f_0 + 2 sum of
+// the even-order values).  The recurrence starts above nmax, so it writes every entry; the
+// caller scales each factor by 1/S as it forms the products (unnormalised values reach 1e250,
+// so their products would overflow).
+__device__ __forceinline__ double miller_rows_unnormalised(int nmax, double z, double* row) {
+  int M = nmax;
+  if ((double)M < z) M = (int)ceil(z);
+  const int N = miller_start(M);
+  const double tox = 2.0 / z;
+  double fkp1 = 0.0, fk = 1e-30, sum = 0.0;
+  for (int k = N; k > 0; --k) {
+    const double fkm1 = ((double)k * tox) * fk - fkp1;
+    fkp1 = fk;
+    fk = fkm1;
+    if (fabs(fk) > 1e250) {
+      fk *= 1e-250;
+      fkp1 *= 1e-250;
+      sum *= 1e-250;
+      for (int i = k; i <= nmax; ++i) row[i] *= 1e-250;
+    }
+    const int km1 = k - 1;
+    if (km1 <= nmax) row[km1] = fk;
+    if (km1 > 0 && (km1 & 1) == 0) sum += fk;
+  }
+  return 1.0 / (2.0 * sum + fk);
+}
+
 template <int TI>
 __global__ void __launch_bounds__(kLocThreads) k_loc_eval_mma(
     const double* __restrict__ ws, double* __restrict__ gs, int ld_gs, int B,
     const LocBoxD* __restrict__ boxes, const EvalItem* __restrict__ items,
     const double* __restrict__ cheb, int K, int nu_int, double sgn, LocEvalMma L) {
-  constexpr int MT = TI / 8;                                      // m-tiles per target tile
-  constexpr int NTW = (MT * (kLocMmaCols / 8) + kLocMmaWarps - 1) / kLocMmaWarps;  // tiles per warp
+  constexpr int MT = TI / 8;                       // m-tiles per target tile
+  constexpr int NTN = kLocMmaCols / 8;             // n-tiles per column pass
+  constexpr int NTW = (MT * NTN + kLocMmaWarps - 1) / kLocMmaWarps;  // tiles per warp
   const EvalItem it = items[blockIdx.x];
   const LocBoxD bx = boxes[it.box];
   const int KL1 = K + 1;
@@ -160,7 +191,11 @@ __global__ void __launch_bounds__(kLocThreads) k_loc_eval_mma(
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* sJ = reinterpret_cast<double*>(smem_raw);  // [TI][JS]
   double* sC = sJ + (size_t)TI * L.JS;                 // [kLocMmaK][CS]
+  __shared__ double s_scale[TI];                       // 1 / S per target of the tile
   const double* cbox = cheb + (size_t)it.box * KL1 * B;
+  // Warp w owns tiles w NTW .. w NTW + NTW - 1 of the MT x NTN tile grid (row-major), so
+  // consecutive tiles of a warp share their m-tile and the left fragment.
+  const int tile0 = warp * NTW;
   for (int i0 = 0; i0 < it.ni; i0 += TI) {
     __syncthreads();  // previous tile's table consumed
     if (tid < TI) {
@@ -170,8 +205,9 @@ __global__ void __launch_bounds__(kLocThreads) k_loc_eval_mma(
       if (z < 1e-30) {
         for (int q = 0; q <= maxo; ++q) row[q] = 0.0;
         row[0] = 1.0;
+        s_scale[tid] = 1.0;
       } else {
-        bessel_j_orders(maxo, z, row);
+        s_scale[tid] = miller_rows_unnormalised(maxo, z, row);
       }
     }
     for (int cb = 0; cb < B; cb += kLocMmaCols) {
@@ -188,33 +224,38 @@ __global__ void __launch_bounds__(kLocThreads) k_loc_eval_mma(
           sC[(size_t)l * L.CS + t] = (l < kn && t < ncol) ? cbox[(size_t)(kc + l) * B + cb + t] : 0.0;
         }
         __syncthreads();
+        for (int k0 = 0; k0 < kn; k0 += 4) {
+          const int l = kc + k0 + ac;  // order of this lane's left element
+          const int lo = l > l0 ? l - l0 : l0 - l;
+          const bool neg = l > l0 && ((l - l0) & 1);
+          const double* bl = sC + (size_t)(k0 + ac) * L.CS + ar;
+          int mt_cur = -1;
+          double a = 0.0;
 #pragma unroll
-        for (int q = 0; q < NTW; ++q) {
-          const int tile = warp + q * kLocMmaWarps;
-          if (tile < MT * (kLocMmaCols / 8)) {
-            const int mt = tile / (kLocMmaCols / 8), nt = tile - mt * (kLocMmaCols / 8);
-            if (nt * 8 < ncol) {
-              const double* jrow = sJ + (size_t)(mt * 8 + ar) * L.JS;
-              for (int k0 = 0; k0 < kn; k0 += 4) {
-                const int l = kc + k0 + ac;  // order of this lane's A element
-                double a = 0.0;
+          for (int q = 0; q < NTW; ++q) {
+            const int tile = tile0 + q;
+            if (tile < MT * NTN) {
+              const int mt = tile / NTN, nt = tile - mt * NTN;
+              if (mt != mt_cur) {  // warp-uniform
+                mt_cur = mt;
+                a = 0.0;
                 if (l < KL1) {
-                  const int lo = l > l0 ? l - l0 : l0 - l;
-                  a = jrow[l0 + odd + l] * jrow[lo];
-                  if (l > l0 && ((l - l0) & 1)) a = -a;
+                  const double* jrow = sJ + (size_t)(mt * 8 + ar) * L.JS;
+                  const double iv = s_scale[mt * 8 + ar];
+                  a = (jrow[l0 + odd + l] * iv) * (jrow[lo] * iv);
+                  if (neg) a = -a;
                 }
-                const double b = sC[(size_t)(k0 + ac) * L.CS + nt * 8 + ar];
-                dmma884(acc[q][0], acc[q][1], a, b);
               }
+              if (nt * 8 < ncol) dmma884(acc[q][0], acc[q][1], a, bl[nt * 8]);
             }
           }
         }
       }
 #pragma unroll
       for (int q = 0; q < NTW; ++q) {
-        const int tile = warp + q * kLocMmaWarps;
-        if (tile >= MT * (kLocMmaCols / 8)) continue;
-        const int mt = tile / (kLocMmaCols / 8), nt = tile - mt * (kLocMmaCols / 8);
+        const int tile = tile0 + q;
+        if (tile >= MT * NTN) continue;
+        const int mt = tile / NTN, nt = tile - mt * NTN;
         const int ii = i0 + mt * 8 + ar;
         const int tt = nt * 8 + 2 * ac;
         if (ii >= it.ni) continue;

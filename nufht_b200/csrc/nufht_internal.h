@@ -32,6 +32,11 @@ struct PlanParams {
   double nu = 0, tol = 0, z_split = 0;
   int K_asy = 0, K_loc = -1;
   double asy_coef[64] = {0};
+  // z_terms[K] (K <= K_asy, integer orders): the table's switch point for K + 1 term pairs at
+  // this order and tolerance -- from there on K + 1 pairs of the Hankel expansion meet tol.
+  // n_z_terms = 0 when unknown (half-integer orders, single boxes with a given K).
+  double z_terms[16] = {0};
+  int n_z_terms = 0;
 };
 
 // Order/tolerance validation and table lookup (fill_plan_parameters,

@@ -52,6 +52,13 @@ int fill_params(double nu, const NufhtOptions& opt, bool extended, PlanParams* P
     if (kv < 0 || kv >= NUFHT_MAX_K) return -6;
     P->K_asy = kv;
     P->z_split = std::isnan(opt.z_split) ? T->z[i_idx][j_idx][kv] : opt.z_split;
+    // switch points of the smaller term counts (entries the tables leave empty are unusable)
+    P->n_z_terms = 0;
+    for (int K = 0; K <= kv && K < 16; ++K) {
+      const double zk = T->z[i_idx][j_idx][K];
+      P->z_terms[K] = zk > 0.0 ? zk : HUGE_VAL;
+    }
+    P->n_z_terms = kv + 1 <= 16 ? kv + 1 : 16;
     P->K_loc = opt.K_loc <= 0 ? T->kw[i_idx][j_idx][kv] : opt.K_loc;
   } else {
     P->K_asy = (int)std::llround(std::fabs(nu) - 0.5);

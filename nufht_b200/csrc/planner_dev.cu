@@ -311,11 +311,46 @@ int device_check_grid(const double* d_a, int len, cudaStream_t st) {
   return h ? -1 : 0;
 }
 
+namespace {
+
+// Initial state of the partition (generate_boxes, :608-657) from the boundary indices
+// {i0, i1, j0, j1}: the local and asymptotic strips around the direct region and the direct
+// region itself as the first level's only box; out_flags[0] = 1 when the rectangle is all
+// local, 2 all asymptotic, 3 when m == 1 or n == 1 (strips only).
+__global__ void k_init_partition(const int* __restrict__ bnd, int m, int n, PartState* st, HBox* dir, HBox* loc,
+                                 HBox* asy, int* out_flags) {
+  if (threadIdx.x != 0) return;
+  const int i0 = bnd[0], i1 = bnd[1], j0 = bnd[2], j1 = bnd[3];
+  int nl = 0, na = 0, flag = 0;
+  if (i0 == -1) {
+    loc[nl++] = HBox{0, n - 1, 0, m - 1};
+    flag = 1;
+  } else if (i1 < 0) {
+    asy[na++] = HBox{0, n - 1, 0, m - 1};
+    flag = 2;
+  } else {
+    if (i0 > 0) loc[nl++] = HBox{0, i0 - 1, 0, m - 1};
+    if (j0 > 0) loc[nl++] = HBox{i0, n - 1, 0, j0 - 1};
+    if (i1 < n - 1) asy[na++] = HBox{i1 + 1, n - 1, 0, m - 1};
+    if (j1 < m - 1) asy[na++] = HBox{0, i1, j1 + 1, m - 1};
+    if (m == 1 || n == 1) flag = 3;
+  }
+  dir[0] = HBox{i0, i1, j0, j1};
+  st->n_dir = flag ? 0 : 1;
+  st->n_loc = nl;
+  st->n_asy = na;
+  st->overflow = 0;
+  out_flags[0] = flag;
+}
+
+}  // namespace
+
 int device_make_boxes(const double* d_rs, int m, const double* d_ws, int n, double z, int max_levels,
-                      int min_dim_prod, int Kthr, HBoxes* out, cudaStream_t st) {
+                      int min_dim_prod, int Kthr, HBoxes* out, cudaStream_t st, int* bad_grid) {
   out->loc.clear();
   out->asy.clear();
   out->dir.clear();
+  if (bad_grid) *bad_grid = 0;
   if (n <= 0 || m <= 0) return 0;
   if (max_levels <= 0) {
     const int mn = std::min(n, m);
@@ -323,97 +358,83 @@ int device_make_boxes(const double* d_rs, int m, const double* d_ws, int n, doub
     max_levels = ratio < 1.0 ? 0 : (int)std::floor(std::log2(ratio));
     if (max_levels < 0) max_levels = 0;
   }
-  DevBuf<int> d_bnd;
-  NUFHT_CUDA_TRY(d_bnd.alloc(4));
-  k_bounds<<<1, 32, 0, st>>>(d_rs, m, d_ws, n, z, d_bnd.p);
-  NUFHT_LAUNCH_CHECK();
-  int bnd[4];
-  NUFHT_CUDA_TRY(cudaMemcpyAsync(bnd, d_bnd.p, sizeof(bnd), cudaMemcpyDeviceToHost, st));
-  NUFHT_CUDA_TRY(cudaStreamSynchronize(st));
-  const int i0 = bnd[0], i1 = bnd[1], j0 = bnd[2], j1 = bnd[3];
-  if (i0 == -1) {
-    out->loc.push_back({0, n - 1, 0, m - 1});
-    return 0;
-  }
-  if (i1 < 0) {
-    out->asy.push_back({0, n - 1, 0, m - 1});
-    return 0;
-  }
-  std::vector<HBox> loc, asy;
-  if (i0 > 0) loc.push_back({0, i0 - 1, 0, m - 1});
-  if (j0 > 0) loc.push_back({i0, n - 1, 0, j0 - 1});
-  if (i1 < n - 1) asy.push_back({i1 + 1, n - 1, 0, m - 1});
-  if (j1 < m - 1) asy.push_back({0, i1, j1 + 1, m - 1});
-  if (m == 1 || n == 1) {
-    out->loc = loc;
-    out->asy = asy;
-    return 0;
-  }
-  // Box buffers start at 64K boxes per list (far above the partitions of the workloads seen:
-  // about a thousand boxes at 1e6 x 1e6) and grow 16-fold when a list overflowed.
-  DevBuf<PartState> dSt;
-  DevBuf<int> dCnt;
-  NUFHT_CUDA_TRY(dSt.alloc(1));
-  NUFHT_CUDA_TRY(dCnt.alloc(3));
-  PartState hs{};
-  DevBuf<HBox> dA, dB, dLoc, dAsy, oLoc, oAsy, oDir;
-  DevBuf<int4> dDec;
-  HBox* cur = nullptr;
+  // One device arena per attempt: the state and small counters, then the box lists.  The lists
+  // start at 64K boxes each (far above the partitions of the workloads seen: about a thousand
+  // boxes at 1e6 x 1e6) and grow 16-fold when one overflowed.
   for (long cap = 1L << 16;; cap *= 16) {
     if (cap > (1L << 28)) {
       std::fprintf(stderr, "nufht_b200: device planner box lists too long\n");
       return NUFHT_E_TOO_LARGE;
     }
-    cudaFree(dA.p); cudaFree(dB.p); cudaFree(dDec.p); cudaFree(dLoc.p); cudaFree(dAsy.p);
-    dA.p = dB.p = dLoc.p = dAsy.p = nullptr;
-    dDec.p = nullptr;
-    NUFHT_CUDA_TRY(dA.alloc(cap));
-    NUFHT_CUDA_TRY(dB.alloc(cap));
-    NUFHT_CUDA_TRY(dDec.alloc(cap));
-    NUFHT_CUDA_TRY(dLoc.alloc(cap));
-    NUFHT_CUDA_TRY(dAsy.alloc(cap));
-    hs = PartState{1, (int)loc.size(), (int)asy.size(), 0};
-    const HBox first{i0, i1, j0, j1};
-    NUFHT_CUDA_TRY(cudaMemcpyAsync(dA.p, &first, sizeof(HBox), cudaMemcpyHostToDevice, st));
-    if (!loc.empty())
-      NUFHT_CUDA_TRY(cudaMemcpyAsync(dLoc.p, loc.data(), sizeof(HBox) * loc.size(), cudaMemcpyHostToDevice, st));
-    if (!asy.empty())
-      NUFHT_CUDA_TRY(cudaMemcpyAsync(dAsy.p, asy.data(), sizeof(HBox) * asy.size(), cudaMemcpyHostToDevice, st));
-    NUFHT_CUDA_TRY(cudaMemcpyAsync(dSt.p, &hs, sizeof(hs), cudaMemcpyHostToDevice, st));
-    cur = dA.p;
-    HBox* nxt = dB.p;
-    for (int lev = 0; lev < max_levels; ++lev) {
-      k_split_level<<<148 * 4, 256, 0, st>>>(d_rs, m, d_ws, z, min_dim_prod, cur, dSt.p, dDec.p);
+    const size_t head = 256;  // PartState, bounds, flags, counts
+    const size_t nb = (size_t)cap;
+    DevBuf<unsigned char> arena;
+    NUFHT_CUDA_TRY(arena.alloc(head + sizeof(HBox) * nb * 8 + sizeof(int4) * nb));
+    unsigned char* a = arena.p;
+    PartState* dSt = reinterpret_cast<PartState*>(a);
+    int* dBnd = reinterpret_cast<int*>(a + 64);      // 4 ints
+    int* dFlag = reinterpret_cast<int*>(a + 96);     // [0] trivial-rectangle flag, [1] bad rs, [2] bad ws
+    int* dCnt = reinterpret_cast<int*>(a + 128);     // final counts
+    HBox* dA = reinterpret_cast<HBox*>(a + head);
+    HBox* dB = dA + nb;
+    HBox* dLoc = dB + nb;
+    HBox* dAsy = dLoc + nb;
+    HBox* oLoc = dAsy + nb;
+    HBox* oAsy = oLoc + nb;
+    HBox* oDir = oAsy + nb;  // 2 nb: the last level's boxes plus reclassified ones
+    int4* dDec = reinterpret_cast<int4*>(oDir + 2 * nb);
+    NUFHT_CUDA_TRY(cudaMemsetAsync(dFlag, 0, 3 * sizeof(int), st));
+    if (bad_grid) {
+      const int br = std::max(1, std::min(148 * 4, (m + 255) / 256)), bw = std::max(1, std::min(148 * 4, (n + 255) / 256));
+      k_check_grid<<<br, 256, 0, st>>>(d_rs, m, dFlag + 1);
       NUFHT_LAUNCH_CHECK();
-      k_emit_level<<<1, kScanThreads, 0, st>>>(cur, dDec.p, dSt.p, nxt, (int)cap, dLoc.p, (int)cap, dAsy.p, (int)cap);
+      k_check_grid<<<bw, 256, 0, st>>>(d_ws, n, dFlag + 2);
+      NUFHT_LAUNCH_CHECK();
+    }
+    k_bounds<<<1, 32, 0, st>>>(d_rs, m, d_ws, n, z, dBnd);
+    NUFHT_LAUNCH_CHECK();
+    k_init_partition<<<1, 32, 0, st>>>(dBnd, m, n, dSt, dA, dLoc, dAsy, dFlag);
+    NUFHT_LAUNCH_CHECK();
+    HBox* cur = dA;
+    HBox* nxt = dB;
+    for (int lev = 0; lev < max_levels; ++lev) {
+      k_split_level<<<148 * 4, 256, 0, st>>>(d_rs, m, d_ws, z, min_dim_prod, cur, dSt, dDec);
+      NUFHT_LAUNCH_CHECK();
+      k_emit_level<<<1, kScanThreads, 0, st>>>(cur, dDec, dSt, nxt, (int)cap, dLoc, (int)cap, dAsy, (int)cap);
       NUFHT_LAUNCH_CHECK();
       std::swap(cur, nxt);
     }
-    NUFHT_CUDA_TRY(cudaMemcpyAsync(&hs, dSt.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    k_classify<<<1, kScanThreads, 0, st>>>(dLoc, dAsy, cur, dSt, Kthr, min_dim_prod, oLoc, oAsy, oDir, dCnt);
+    NUFHT_LAUNCH_CHECK();
+    struct {
+      PartState s;    // offset 0
+      int pad[20];
+      int flag[3];    // offset 96
+      int pad2[5];
+      int cnt[3];     // offset 128
+    } h;
+    static_assert(sizeof(PartState) == 16 && sizeof(h) == 140, "arena layout");
+    NUFHT_CUDA_TRY(cudaMemcpyAsync(&h, a, sizeof(h), cudaMemcpyDeviceToHost, st));
     NUFHT_CUDA_TRY(cudaStreamSynchronize(st));
-    if (!hs.overflow) break;
+    if (h.flag[1] || h.flag[2]) {
+      if (bad_grid) *bad_grid = h.flag[1] ? 1 : 2;
+      return 0;
+    }
+    if (h.s.overflow) continue;
+    const int cl = h.flag[0] == 0 ? h.cnt[0] : h.s.n_loc;
+    const int ca = h.flag[0] == 0 ? h.cnt[1] : h.s.n_asy;
+    const int cd = h.flag[0] == 0 ? h.cnt[2] : 0;
+    const HBox* sl = h.flag[0] == 0 ? oLoc : dLoc;
+    const HBox* sa = h.flag[0] == 0 ? oAsy : dAsy;
+    out->loc.resize(cl);
+    out->asy.resize(ca);
+    out->dir.resize(cd);
+    if (cl) NUFHT_CUDA_TRY(cudaMemcpyAsync(out->loc.data(), sl, sizeof(HBox) * cl, cudaMemcpyDeviceToHost, st));
+    if (ca) NUFHT_CUDA_TRY(cudaMemcpyAsync(out->asy.data(), sa, sizeof(HBox) * ca, cudaMemcpyDeviceToHost, st));
+    if (cd) NUFHT_CUDA_TRY(cudaMemcpyAsync(out->dir.data(), oDir, sizeof(HBox) * cd, cudaMemcpyDeviceToHost, st));
+    NUFHT_CUDA_TRY(cudaStreamSynchronize(st));
+    return 0;
   }
-  const long tot = (long)hs.n_dir + hs.n_loc + hs.n_asy;
-  NUFHT_CUDA_TRY(oLoc.alloc(hs.n_loc));
-  NUFHT_CUDA_TRY(oAsy.alloc(hs.n_asy));
-  NUFHT_CUDA_TRY(oDir.alloc(tot));
-  k_classify<<<1, kScanThreads, 0, st>>>(dLoc.p, dAsy.p, cur, dSt.p, Kthr, min_dim_prod, oLoc.p, oAsy.p, oDir.p,
-                                         dCnt.p);
-  NUFHT_LAUNCH_CHECK();
-  int cnt[3];
-  NUFHT_CUDA_TRY(cudaMemcpyAsync(cnt, dCnt.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
-  NUFHT_CUDA_TRY(cudaStreamSynchronize(st));
-  out->loc.resize(cnt[0]);
-  out->asy.resize(cnt[1]);
-  out->dir.resize(cnt[2]);
-  if (cnt[0])
-    NUFHT_CUDA_TRY(cudaMemcpyAsync(out->loc.data(), oLoc.p, sizeof(HBox) * cnt[0], cudaMemcpyDeviceToHost, st));
-  if (cnt[1])
-    NUFHT_CUDA_TRY(cudaMemcpyAsync(out->asy.data(), oAsy.p, sizeof(HBox) * cnt[1], cudaMemcpyDeviceToHost, st));
-  if (cnt[2])
-    NUFHT_CUDA_TRY(cudaMemcpyAsync(out->dir.data(), oDir.p, sizeof(HBox) * cnt[2], cudaMemcpyDeviceToHost, st));
-  NUFHT_CUDA_TRY(cudaStreamSynchronize(st));
-  return 0;
 }
 
 }  // namespace hankel

@@ -10,7 +10,7 @@ namespace hankel {
 
 // out[0]  sum over asymptotic boxes of sources (nj)
 // out[1]  sum over asymptotic boxes of targets (ni)
-// out[2]  FFT cells (sum of n2)
+// out[2]  FFT cells (sum of n2; entries 2-4, 8, 9 in units of NLP-term vectors)
 // out[3]  sum of nj * W (spreading taps per vector)
 // out[4]  sum of ni * W (interpolation taps per vector)
 // out[5]  direct-box pairs (sum of ni * nj)
@@ -29,16 +29,19 @@ namespace hankel {
 // out[18] 1 when the box partition ran on the device
 void plan_stats(const DevicePlan& D, double* out, int n) {
   double s[19] = {0};
+  // Per-vector sums (entries 2-4, 8, 9) count a box with fewer expansion terms than the
+  // plan's NLP in proportion (nlp / NLP), so that multiplying by NLP * B gives the work.
   for (const AsyBoxD& b : D.asyb) {
     double nj = b.j1 - b.j0 + 1, ni = b.i1 - b.i0 + 1;
     const AsyClass& K = D.classes[b.cls];
+    const double f = D.NLP > 0 ? (double)b.nlp / (double)D.NLP : 1.0;
     s[0] += nj;
     s[1] += ni;
-    s[2] += b.n2;
-    s[3] += nj * K.W;
-    s[4] += ni * K.W;
-    s[8] += std::min((double)b.n2, b.n2 / K.sigma + K.W);
-    s[9] += 5.0 * b.n2 * std::log2((double)b.n2);
+    s[2] += f * b.n2;
+    s[3] += f * nj * K.W;
+    s[4] += f * ni * K.W;
+    s[8] += f * std::min((double)b.n2, b.n2 / K.sigma + K.W);
+    s[9] += f * 5.0 * b.n2 * std::log2((double)b.n2);
     if (K.sigma != 2.0) s[12] += 1.0;
   }
   for (const HBox& b : D.dir_boxes) s[5] += (double)(b.i1 - b.i0 + 1) * (double)(b.j1 - b.j0 + 1);

@@ -143,6 +143,7 @@ def test_module_reuses_plans(cuda):
     plans = mod._plans
     g2 = mod(c, r, k)
     assert mod._plans is plans
-    assert torch.equal(g1, g2)
+    # the phases add into g with atomics from concurrent streams: equal up to summation order
+    assert torch.allclose(g1, g2, rtol=0, atol=1e-13 * float(g1.abs().max()))
     g2.sum().backward()
     assert c.grad is not None and c.grad.shape == c.shape
