@@ -6,6 +6,7 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "executor.h"
 #include "kernels_asy.cuh"
@@ -25,31 +26,44 @@ AsyShape asy_shape(int NLP, int B, int LPT) {
   return L;
 }
 
-template <typename T, int W, int LPT, bool WINDOWED>
+template <typename T, int W, int LPT, bool WINDOWED, bool DIRECT>
 int launch_spread_kind(DevicePlan& D, const AsyClass& K, int item0, int nitems, const double* cs, int ld_cs,
                        int B, cudaStream_t st) {
   if (nitems == 0) return 0;
   const AsyShape L = asy_shape(K.ac.NLP, B, LPT);
-  size_t sm = spread_smem<T>(W, L.BT * K.ac.NLP, L.NG, L.BT, WINDOWED, spread_tile_cells(K.ac.NLP)).total;
+  size_t sm = spread_smem<T>(W, L.BT * K.ac.NLP, L.NG, L.BT, WINDOWED && !DIRECT, K.ac.tile_cells).total;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(k_asy_spread<T, W, LPT, WINDOWED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_asy_spread<T, W, LPT, WINDOWED, DIRECT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          220 * 1024);
     attr_set = true;
   }
   dim3 g((unsigned)nitems, (unsigned)L.ngy);
-  k_asy_spread<T, W, LPT, WINDOWED><<<g, L.threads, sm, st>>>(
+  k_asy_spread<T, W, LPT, WINDOWED, DIRECT><<<g, L.threads, sm, st>>>(
       D.d_rs, cs, ld_cs, B, (typename Cplx<T>::type*)D.d_grid, D.d_asyb, D.d_spread + item0, D.d_corr, K.ac,
       L.BT, L.V_total);
   NUFHT_LAUNCH_CHECK();
   return 0;
 }
 
+// Tiles store finished cells straight to the grid (each CTA owns its cells, so no atomics)
+// rather than through a shared window written out at the end: without the window more CTAs
+// fit on an SM, and L2 merges the scattered 8- or 16-byte stores of consecutive cells.
+// NUFHT_B200_SPREAD_DIRECT=0 selects the window form.
+inline bool spread_direct() {
+  static const bool on = [] {
+    const char* e = std::getenv("NUFHT_B200_SPREAD_DIRECT");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 template <typename T, int W, int LPT>
 int launch_spread_lpt(DevicePlan& D, const AsyClass& K, const double* cs, int ld_cs, int B, cudaStream_t st) {
-  int rc = launch_spread_kind<T, W, LPT, true>(D, K, K.spread0, K.nspread, cs, ld_cs, B, st);
+  int rc = spread_direct() ? launch_spread_kind<T, W, LPT, true, true>(D, K, K.spread0, K.nspread, cs, ld_cs, B, st)
+                           : launch_spread_kind<T, W, LPT, true, false>(D, K, K.spread0, K.nspread, cs, ld_cs, B, st);
   if (rc) return rc;
-  return launch_spread_kind<T, W, LPT, false>(D, K, K.spreadA0, K.nspreadA, cs, ld_cs, B, st);
+  return launch_spread_kind<T, W, LPT, false, false>(D, K, K.spreadA0, K.nspreadA, cs, ld_cs, B, st);
 }
 
 template <typename T, int W, int LPT>
@@ -73,10 +87,19 @@ int launch_interp_lpt(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, i
 // Terms per thread (register blocking): LPT = 2, or 1 in double precision for windows wider
 // than 10 (register budget) and for classes of at most 4 terms (so that a CTA keeps at least
 // two warps' worth of threads, NLP / LPT per column); NLP = 2 (K + 1) is even.
+// NUFHT_B200_LPT_SMALL=2 keeps two terms per thread for classes of at most 4 terms.
+inline int lpt_small() {
+  static const int v = [] {
+    const char* e = std::getenv("NUFHT_B200_LPT_SMALL");
+    return (e && e[0] == '2') ? 2 : 1;
+  }();
+  return v;
+}
+
 template <typename T, int W>
 int launch_spread(DevicePlan& D, const AsyClass& K, const double* cs, int ld_cs, int B, cudaStream_t st) {
   if constexpr (sizeof(T) == 8 && W > 10) return launch_spread_lpt<T, W, 1>(D, K, cs, ld_cs, B, st);
-  else if (K.ac.NLP <= 4) return launch_spread_lpt<T, W, 1>(D, K, cs, ld_cs, B, st);
+  else if (K.ac.NLP <= 4 && lpt_small() == 1) return launch_spread_lpt<T, W, 1>(D, K, cs, ld_cs, B, st);
   else return launch_spread_lpt<T, W, 2>(D, K, cs, ld_cs, B, st);
 }
 
@@ -85,7 +108,7 @@ template <typename T, int W>
 int launch_interp(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, int B, cudaStream_t st, double sgn) {
   if (K.ninterp == 0) return 0;
   if constexpr (sizeof(T) == 8 && W > 10) return launch_interp_lpt<T, W, 1>(D, K, gs, ld_gs, B, st, sgn);
-  else if (K.ac.NLP <= 4) return launch_interp_lpt<T, W, 1>(D, K, gs, ld_gs, B, st, sgn);
+  else if (K.ac.NLP <= 4 && lpt_small() == 1) return launch_interp_lpt<T, W, 1>(D, K, gs, ld_gs, B, st, sgn);
   else return launch_interp_lpt<T, W, 2>(D, K, gs, ld_gs, B, st, sgn);
 }
 

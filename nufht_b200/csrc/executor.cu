@@ -639,7 +639,10 @@ void DevicePlan::build_lists() {
     K.nspreadA = (int)atomic_items.size();
     atomic_items.clear();
     K.ninterp = (int)interp.size() - K.interp0;
-    if (any) K.ac = make_asy_const(P, K.nlp, K.W, es_beta(K.sigma, K.W));
+    if (any) {
+      K.ac = make_asy_const(P, K.nlp, K.W, es_beta(K.sigma, K.W));
+      K.ac.tile_cells = spread_tile_cells(K.nlp);
+    }
     else std::memset(&K.ac, 0, sizeof(K.ac));
     classes.push_back(K);
   }
@@ -888,31 +891,31 @@ int launch_loc_eval_t(const double* ws, double* gs, int ld_gs, int B, const LocB
   return 0;
 }
 
-// Projection on the FP64 tensor cores (k_loc_proj_mma): columns per CTA and staged sources
-// per round chosen so that the output tiles fit the warps' registers and the tables the
-// shared-memory budget.  Returns 1 when the degree is too large for it (SIMT path then).
+// Projection on the FP64 tensor cores (k_loc_proj_mma): CTAs of (source chunk item, block
+// of up to 128 orders, block of up to 64 columns), so that every table entry a CTA fills
+// serves all its columns; staged sources per round chosen for the shared-memory budget.
+// Returns 1 when the layout does not fit (SIMT path then).
 int launch_loc_proj_mma(const double* rs, const double* cs, int ld_cs, int B, const LocBoxD* d_box,
                         const ProjItem* d_proj, int nproj, double* d_partial, int KL1, int odd, cudaStream_t st) {
-  const int nmt = round8(KL1) / 8;
-  int BT = std::min(32, round8(B));
-  while (BT > 8 && nmt * (BT / 8) > kLocMmaWarps * 4) BT -= 8;
-  const int tiles = nmt * (BT / 8);
+  const int MB = std::min(128, round8(KL1));
+  const int BT = std::min(64, round8(B));
+  const int tiles = (MB / 8) * (BT / 8);
   if (tiles > kLocMmaWarps * 16) return 1;
   int chunk = 128;
-  LocProjMma L = loc_proj_mma_layout(KL1, BT, chunk);
-  while (chunk > 4 && L.doubles() > kLocSmemDoubles) {
+  LocProjMma L = loc_proj_mma_layout(MB, BT, chunk);
+  while (chunk > 4 && L.doubles() > (size_t)(100 * 1024 / 8)) {
     chunk -= 4;
-    L = loc_proj_mma_layout(KL1, BT, chunk);
+    L = loc_proj_mma_layout(MB, BT, chunk);
   }
   if (L.doubles() > kLocSmemDoubles) return 1;
   const size_t sm = sizeof(double) * L.doubles();
-  dim3 g((unsigned)nproj, (unsigned)((B + BT - 1) / BT));
+  dim3 g((unsigned)nproj, (unsigned)((KL1 + MB - 1) / MB), (unsigned)((B + BT - 1) / BT));
   if (tiles <= kLocMmaWarps * 4) {
     if (sm > 48 * 1024) cudaFuncSetAttribute(k_loc_proj_mma<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_loc_proj_mma<4><<<g, kLocThreads, sm, st>>>(rs, cs, ld_cs, B, d_box, d_proj, KL1, odd, d_partial, BT, L);
+    k_loc_proj_mma<4><<<g, kLocThreads, sm, st>>>(rs, cs, ld_cs, B, d_box, d_proj, KL1, odd, d_partial, L);
   } else {
     if (sm > 48 * 1024) cudaFuncSetAttribute(k_loc_proj_mma<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_loc_proj_mma<16><<<g, kLocThreads, sm, st>>>(rs, cs, ld_cs, B, d_box, d_proj, KL1, odd, d_partial, BT, L);
+    k_loc_proj_mma<16><<<g, kLocThreads, sm, st>>>(rs, cs, ld_cs, B, d_box, d_proj, KL1, odd, d_partial, L);
   }
   NUFHT_LAUNCH_CHECK();
   return 0;
@@ -937,15 +940,18 @@ int launch_loc_eval_mma(const double* ws, double* gs, int ld_gs, int B, const Lo
                         int neval, const double* d_cheb, int K, int nu_int, double sgn, cudaStream_t st) {
   const int maxo = nu_int / 2 + K + (nu_int & 1);
   // The tile with the most targets resident per SM (shared memory decides how many CTAs
-  // fit); ties go to the larger tile, which stages the coefficients for more targets.
+  // fit); at equal counts the one with more CTAs per SM, so that one CTA's Bessel recurrences
+  // overlap another's products.
   const int tis[4] = {128, 32, 16, 8};
-  int pick = -1, best = 0;
+  int pick = -1, best = 0, best_ctas = 0;
   for (int q = 0; q < 4; ++q) {
     const size_t bytes = sizeof(double) * loc_eval_mma_layout(tis[q], maxo).doubles();
     if (bytes > sizeof(double) * kLocSmemDoubles) continue;
-    const int per_sm = tis[q] * (int)std::min<size_t>(8, (size_t)(224 * 1024) / (bytes + 1024));
-    if (per_sm > best) {
+    const int ctas = (int)std::min<size_t>(8, (size_t)(224 * 1024) / (bytes + 1024));
+    const int per_sm = tis[q] * ctas;
+    if (per_sm > best || (per_sm == best && ctas > best_ctas)) {
       best = per_sm;
+      best_ctas = ctas;
       pick = tis[q];
     }
   }

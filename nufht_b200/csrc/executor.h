@@ -61,6 +61,7 @@ struct FftGroup {
 
 struct AsyConst {
   int NLP;      // 2 (K + 1)
+  int tile_cells;  // cells of a mode-0 spreading tile of this class
   int nq;       // quadrature nodes
   double beta;  // kernel shape
   double cos_phi, sin_phi;  // exp(i pi (-nu/2 - 1/4))

@@ -23,6 +23,7 @@
 #pragma once
 
 #include <climits>
+#include <cstdlib>
 
 #include "kernels_common.cuh"
 
@@ -65,11 +66,19 @@ struct AsyShape {
   int LPT, NG, BT, threads, ngy, V_total;
 };
 
-// Cells of a mode-0 spreading tile: 16 at 6 or more expansion terms, 32 at 2 or 4 (whose
-// CTAs have one term per thread, NLP / 1 threads per column).  The shared window of a tile
-// (cells x (vectors + 1) complex values) decides how many CTAs fit on an SM: these sizes keep
-// it near 16 KB for 2 and 4 terms and 33 KB for 8, at least 16 warps per SM either way.
-__host__ __device__ constexpr int spread_tile_cells(int nlp) { return nlp >= 6 ? kSpreadTile : 2 * kSpreadTile; }
+// Cells of a mode-0 spreading tile (AsyConst::tile_cells, chosen per kernel class at plan
+// time): 16 at 6 or more expansion terms, 32 at 2 or 4 (whose CTAs have one term per thread,
+// NLP / 1 threads per column), or NUFHT_B200_TILE_CELLS_SMALL for 2 and 4 terms.  A window
+// (cells x (vectors + 1) complex values, when tiles write through shared memory) of these
+// sizes stays near 16 KB for 2 and 4 terms and 33 KB for 8.
+inline int spread_tile_cells(int nlp) {
+  static const int small = [] {
+    const char* e = std::getenv("NUFHT_B200_TILE_CELLS_SMALL");
+    const int v = e ? std::atoi(e) : 0;
+    return (v >= 8 && v <= 256) ? v : 2 * kSpreadTile;
+  }();
+  return nlp >= 6 ? kSpreadTile : small;
+}
 
 // Staged kernel weights per source (complex) and per target (real), padded so that every
 // row is read with 16-byte shared-memory loads.
@@ -220,7 +229,7 @@ __device__ __forceinline__ void grid_atomic_add(double2* p, double2 v) {
 // atomically to the pre-zeroed grid (mode-1 source chunks of dense boxes).  Empty stretches
 // between sources are skipped once the ring is empty.  The source phase exp(i D x) is folded
 // into complex kernel weights staged once per source.
-template <typename T, int W, int LPT, bool WINDOWED>
+template <typename T, int W, int LPT, bool WINDOWED, bool DIRECT = false>
 __global__ void __launch_bounds__(256) k_asy_spread(
     const double* __restrict__ rs, const double* __restrict__ cs, int ld_cs, int B,
     typename Cplx<T>::type* __restrict__ grid, const AsyBoxD* __restrict__ boxes,
@@ -255,8 +264,8 @@ __global__ void __launch_bounds__(256) k_asy_spread(
   }
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int TC = spread_tile_cells(NLP);
-  const SpreadSmem L = spread_smem<T>(W, VCTA, NG, BT, WINDOWED, TC);
+  const int TC = P.tile_cells;
+  const SpreadSmem L = spread_smem<T>(W, VCTA, NG, BT, WINDOWED && !DIRECT, TC);
   C2* win = reinterpret_cast<C2*>(smem_raw + L.win);        // [TC][WP]
   C2* s_wc = reinterpret_cast<C2*>(smem_raw + L.wc);        // [SCH][WE]
   C2* s_rq = reinterpret_cast<C2*>(smem_raw + L.rq);        // [SCH][NG]: (rho of term g LPT, rref / r)
@@ -266,7 +275,7 @@ __global__ void __launch_bounds__(256) k_asy_spread(
   int* s_l0 = reinterpret_cast<int*>(smem_raw + L.l0);      // [SCH]
   int* s_end = reinterpret_cast<int*>(smem_raw + L.end);    // [SCH]: end of the equal-l0 run
 
-  if (WINDOWED)
+  if (WINDOWED && !DIRECT)
     for (int e = tid; e < TC * WP; e += nthr) win[e] = cmake<T>(0, 0);
   const T ihw = (T)(2.0 / (double)W);
   const T beta = (T)P.beta;
@@ -295,9 +304,15 @@ __global__ void __launch_bounds__(256) k_asy_spread(
       s_c[tt * SCP + s] = (T)((t0 + tt < B) ? cs[(size_t)(t0 + tt) * ld_cs + s0 + s] : 0.0);
     }
     __syncthreads();
+    // complex weights psi(l - u) exp(i D x) / psi-hat(cell l): the deconvolution factor of the
+    // target cell is folded in here (loaded in parallel with the other weights), so finished
+    // cells are stored as they are
     for (int e = tid; e < ns * WE; e += nthr) {
       int s = e / WE, q = e - s * WE;
-      T w = q < W ? es_kernel_t((T)((double)(s_l0[s] + q) - s_u[s]), ihw, beta) : (T)0;
+      const int cell = s_l0[s] + q;
+      T w = (q < W && cell >= -bx.half && cell <= bx.half)
+                ? es_kernel_t((T)((double)cell - s_u[s]), ihw, beta) * (T)corr[bx.corr_off + cell + bx.half]
+                : (T)0;
       C2 ph = s_ph[s];
       s_wc[e] = cmake<T>(w * ph.x, w * ph.y);
     }
@@ -310,6 +325,21 @@ __global__ void __launch_bounds__(256) k_asy_spread(
   for (int u = 0; u < LPT; ++u)
 #pragma unroll
     for (int q = 0; q < W; ++q) acc[u][q] = cmake<T>(0, 0);
+
+  // DIRECT tiles write every cell they own exactly once, in increasing order: cells the walk
+  // skips (no source support) get zeros.  zc = first owned cell not written yet.
+  int zc = it.l_start;
+  auto zero_to = [&](int upto) {  // zeros for owned cells [zc, upto)
+    if (!(WINDOWED && DIRECT)) return;
+    const int hi = min(upto, it.l_start + nc);
+    if (active)
+      for (int cc = max(zc, it.l_start); cc < hi; ++cc) {
+        const int idx = it.fft_start + (cc - it.l_start);
+#pragma unroll
+        for (int u = 0; u < LPT; ++u) gbox[(size_t)(v0 + vloc + u) * bx.n2 + idx] = cmake<T>(0, 0);
+      }
+    zc = max(zc, hi);
+  };
 
   if (it.je > it.js) {
     int s0 = it.js;
@@ -365,17 +395,25 @@ __global__ void __launch_bounds__(256) k_asy_spread(
           if (WINDOWED) {
             const int cl = c - it.l_start;
             if (cl >= 0 && cl < nc) {
+              if (DIRECT) {
+                // the CTA owns the cell: zeros for the owned cells skipped before it, then
+                // the cell scaled by 1/psi-hat, for each vector
+                zero_to(c);
+                zc = c + 1;
+                const int idx = it.fft_start + cl;
 #pragma unroll
-              for (int u = 0; u < LPT; ++u) win[cl * WP + vloc + u] = acc[u][jj];
+                for (int u = 0; u < LPT; ++u) gbox[(size_t)(v0 + vloc + u) * bx.n2 + idx] = acc[u][jj];
+              } else {
+#pragma unroll
+                for (int u = 0; u < LPT; ++u) win[cl * WP + vloc + u] = acc[u][jj];
+              }
             }
           } else if (c >= -bx.half && c <= bx.half) {
-            const T cf = (T)corr[bx.corr_off + c + bx.half];
             const int idx = c < 0 ? c + bx.n2 : c;
 #pragma unroll
             for (int u = 0; u < LPT; ++u) {
               const C2 v = acc[u][jj];
-              if (v.x != (T)0 || v.y != (T)0)
-                grid_atomic_add(gbox + (size_t)(v0 + vloc + u) * bx.n2 + idx, cmake<T>(v.x * cf, v.y * cf));
+              if (v.x != (T)0 || v.y != (T)0) grid_atomic_add(gbox + (size_t)(v0 + vloc + u) * bx.n2 + idx, v);
             }
           }
         }
@@ -393,15 +431,14 @@ __global__ void __launch_bounds__(256) k_asy_spread(
       }
     }
   }
-  if (!WINDOWED) return;
+  zero_to(INT_MAX);  // owned cells after the walk (or all of them when no source reaches the tile)
+  if (!WINDOWED || DIRECT) return;
   __syncthreads();
   // Transposed write-out of the CTA's own cells: consecutive threads take consecutive
   // cells of one vector.
   for (int e = tid; e < nc * nv; e += nthr) {
     int vv = e / nc, cell = e - vv * nc;
-    C2 val = win[cell * WP + vv];
-    T cf = (T)corr[bx.corr_off + it.l_start + cell + bx.half];
-    gbox[(size_t)(v0 + vv) * bx.n2 + it.fft_start + cell] = cmake<T>(val.x * cf, val.y * cf);
+    gbox[(size_t)(v0 + vv) * bx.n2 + it.fft_start + cell] = win[cell * WP + vv];
   }
 }
 
@@ -558,13 +595,17 @@ __global__ void __launch_bounds__(256) k_asy_interp(
         // the slot of cell c takes cell c + R (one cell ahead of the next stencil)
 #pragma unroll
         for (int u = 0; u < LPT; ++u) gw[u][jj] = fetch(c + R, u);
+        c = nxt;
       } else {
+        // a jump: refill the ring in its canonical order and restart at position 0 (one
+        // refill sequence in the code instead of one per ring position)
 #pragma unroll
         for (int q = 0; q < R; ++q)
 #pragma unroll
-          for (int u = 0; u < LPT; ++u) gw[u][(jj + 1 + q) % R] = fetch(nxt + q, u);
+          for (int u = 0; u < LPT; ++u) gw[u][q] = fetch(nxt + q, u);
+        c = nxt;
+        break;
       }
-      c = nxt;
     }
   }
 }

@@ -30,84 +30,103 @@ __host__ __device__ constexpr int stride4(int v) { return v + ((4 - v) % 16 + 16
 
 constexpr int kLocMmaWarps = kLocThreads / 32;
 
-// Shared-memory layout of k_loc_proj_mma (doubles): the table T[MT8][TS] then c[chunk][BS].
+// Shared-memory layout of k_loc_proj_mma (doubles): the table T[MB][TS] of the CTA's block
+// of orders, then c[chunk][BS] of its block of columns.
 struct LocProjMma {
-  int MT8, TS, BS, chunk;
-  __host__ __device__ size_t doubles() const { return (size_t)MT8 * TS + (size_t)chunk * BS; }
+  int MB, BT, TS, BS, chunk;
+  __host__ __device__ size_t doubles() const { return (size_t)MB * TS + (size_t)chunk * BS; }
 };
-inline LocProjMma loc_proj_mma_layout(int KL1, int BT, int chunk) {
+inline LocProjMma loc_proj_mma_layout(int MB, int BT, int chunk) {
   LocProjMma L;
-  L.MT8 = round8(KL1);
+  L.MB = MB;
+  L.BT = BT;
   L.chunk = chunk;
   L.TS = stride4(chunk);
   L.BS = stride4(round8(BT));
   return L;
 }
 
-// Projection of one source chunk item onto the Chebyshev polynomials, BT columns per CTA.
-// Warp w owns the output tiles w, w + 8, ... (at most NT) of the (MT8/8) x (BT8/8) tile grid.
+// Projection of one source chunk item onto the Chebyshev polynomials.  CTA (item, order block
+// ob, column block) covers orders [ob MB, ob MB + MB) and BT columns: it fills only its own
+// orders of the table (segments seeded with cos(m theta), see k_loc_proj) and reuses every
+// table entry for all BT columns.  Warp w owns the output tiles w, w + 8, ... (at most NT) of the
+// (MB/8) x (BT/8) tile grid, strided (tile = w + 8 q): a warp's tiles share their n-tile.
 template <int NT>
 __global__ void __launch_bounds__(kLocThreads) k_loc_proj_mma(
     const double* __restrict__ rs, const double* __restrict__ cs, int ld_cs, int B,
     const LocBoxD* __restrict__ boxes, const ProjItem* __restrict__ items, int KL1, int odd,
-    double* __restrict__ partial, int BT, LocProjMma L) {
+    double* __restrict__ partial, LocProjMma L) {
   const ProjItem it = items[blockIdx.x];
   const LocBoxD bx = boxes[it.box];
-  const int t0 = blockIdx.y * BT;
+  const int lb = blockIdx.y * L.MB;               // first order of the block
+  const int nl = min(L.MB, KL1 - lb);             // orders of the block
+  const int t0 = blockIdx.z * L.BT;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* sT = reinterpret_cast<double*>(smem_raw);  // [MT8][TS]
-  double* sC = sT + (size_t)L.MT8 * L.TS;              // [chunk][BS]
+  double* sT = reinterpret_cast<double*>(smem_raw);  // [MB][TS]
+  double* sC = sT + (size_t)L.MB * L.TS;               // [chunk][BS]
   const int chunk = L.chunk;
-  const int nnt = round8(BT) >> 3;
-  const int ntiles = (L.MT8 >> 3) * nnt;
+  const int nnt = round8(L.BT) >> 3;
+  const int ntiles = (round8(nl) >> 3) * nnt;
   double acc[NT][2];
+  int a_off[NT], b_off[NT];  // this lane's fragment offsets of each tile (-1: no tile)
 #pragma unroll
-  for (int q = 0; q < NT; ++q) acc[q][0] = acc[q][1] = 0.0;
-  // padded orders KL1 .. MT8-1 stay zero
-  for (int e = tid; e < (L.MT8 - KL1) * L.TS; e += blockDim.x) sT[(size_t)KL1 * L.TS + e] = 0.0;
+  for (int q = 0; q < NT; ++q) {
+    acc[q][0] = acc[q][1] = 0.0;
+    const int tile = warp + q * kLocMmaWarps;
+    const int mt = tile / nnt, nt = tile - mt * nnt;
+    a_off[q] = tile < ntiles ? mt * 8 * L.TS : -1;
+    b_off[q] = nt * 8;
+  }
+  // orders of the block past KL1 (padding to whole m-tiles) stay zero
+  for (int e = tid; e < (L.MB - nl) * L.TS; e += blockDim.x) sT[(size_t)nl * L.TS + e] = 0.0;
   const double inv_end = bx.r_end > 0.0 ? 1.0 / bx.r_end : 0.0;
-  const int nseg = (KL1 + kLocSeg - 1) / kLocSeg;
+  const int nseg = (nl + kLocSeg - 1) / kLocSeg;
+  const int ar = lane >> 2, ac = lane & 3;
   for (int s0 = 0; s0 < it.nj; s0 += chunk) {
     const int ns = min(chunk, it.nj - s0);
     __syncthreads();  // previous chunk consumed
     for (int e = tid; e < nseg * chunk; e += blockDim.x) {
       const int sg = e / chunk, s = e - sg * chunk;
-      const int l0 = sg * kLocSeg, l1 = min(KL1, l0 + kLocSeg);
+      const int la = sg * kLocSeg, le = min(nl, la + kLocSeg);  // block-relative orders
       if (s < ns) {
         double x = rs[it.j0 + s0 + s] * inv_end;
         x = fmin(fmax(x, -1.0), 1.0);
         const double th = acos(x);
-        const int m0 = odd ? 2 * l0 + 1 : 2 * l0;
+        const int m0 = odd ? 2 * (lb + la) + 1 : 2 * (lb + la);  // degree of order lb + la
         double tp = cos((double)(m0 - 2) * th);
         double tc = cos((double)m0 * th);
         const double two_t2 = 2.0 * (2.0 * x * x - 1.0);
-        for (int l = l0; l < l1; ++l) {
-          sT[(size_t)l * L.TS + s] = (odd || l > 0) ? 2.0 * tc : tc;
+        for (int l = la; l < le; ++l) {
+          sT[(size_t)l * L.TS + s] = (odd || lb + l > 0) ? 2.0 * tc : tc;
           const double tn = two_t2 * tc - tp;
           tp = tc;
           tc = tn;
         }
       } else {
-        for (int l = l0; l < l1; ++l) sT[(size_t)l * L.TS + s] = 0.0;
+        for (int l = la; l < le; ++l) sT[(size_t)l * L.TS + s] = 0.0;
       }
     }
     for (int e = tid; e < chunk * L.BS; e += blockDim.x) {
       const int s = e / L.BS, tt = e - s * L.BS;
-      sC[e] = (s < ns && tt < BT && t0 + tt < B) ? cs[(size_t)(t0 + tt) * ld_cs + it.j0 + s0 + s] : 0.0;
+      sC[e] = (s < ns && tt < L.BT && t0 + tt < B) ? cs[(size_t)(t0 + tt) * ld_cs + it.j0 + s0 + s] : 0.0;
     }
     __syncthreads();
-    const int ar = lane >> 2, ac = lane & 3;
-    // sources outer, tiles inner: the warp's NT accumulator chains advance together
+    // sources outer, tiles inner: the warp's NT accumulator chains advance together, and
+    // consecutive tiles of a warp reuse the left fragment of their m-tile
     for (int k0 = 0; k0 < chunk; k0 += 4) {
       const double* pa = sT + (size_t)ar * L.TS + k0 + ac;
       const double* pb = sC + (size_t)(k0 + ac) * L.BS + ar;
+      int b_cur = -1;
+      double b = 0.0;
 #pragma unroll
       for (int q = 0; q < NT; ++q) {
-        const int tile = warp + q * kLocMmaWarps;
-        if (tile < ntiles) {
-          const int mt = tile / nnt, nt = tile - mt * nnt;
-          dmma884(acc[q][0], acc[q][1], pa[(size_t)mt * 8 * L.TS], pb[nt * 8]);
+        if (a_off[q] >= 0) {  // warp-uniform
+          if (b_off[q] != b_cur) {  // constant over q when the n-tile count divides 8
+            b_cur = b_off[q];
+            b = pb[b_cur];
+          }
+          dmma884(acc[q][0], acc[q][1], pa[a_off[q]], b);
         }
       }
     }
@@ -117,11 +136,11 @@ __global__ void __launch_bounds__(kLocThreads) k_loc_proj_mma(
     const int tile = warp + q * kLocMmaWarps;
     if (tile >= ntiles) continue;
     const int mt = tile / nnt, nt = tile - mt * nnt;
-    const int l = mt * 8 + (lane >> 2);
+    const int l = lb + mt * 8 + (lane >> 2);
     const int tt = nt * 8 + 2 * (lane & 3);
 #pragma unroll
     for (int h = 0; h < 2; ++h)
-      if (l < KL1 && tt + h < BT && t0 + tt + h < B)
+      if (l < KL1 && tt + h < L.BT && t0 + tt + h < B)
         partial[((size_t)blockIdx.x * KL1 + l) * B + t0 + tt + h] = acc[q][h];
   }
 }
@@ -151,6 +170,26 @@ inline LocEvalMma loc_eval_mma_layout(int TI, int maxo) {
 // caller scales each factor by 1/S as it forms the products (unnormalised values reach 1e250,
 // so their products would overflow).
 __device__ __forceinline__ double miller_rows_unnormalised(int nmax, double z, double* row) {
+  // Orders far above z underflow: |J_n(z)| <= (z/2)^n / n!, below 1e-300 from some n_eff on.
+  // Those entries are zero (their products with |J| <= 1 are below FP64's range), and the
+  // recurrence starts above n_eff instead of nmax -- at small z a start at nmax would grow by
+  // ~2n/z per step and rescale the whole row every few dozen steps.
+  int neff = nmax;
+  if (z < (double)nmax) {
+    const double lz = log(0.5 * z);
+    auto lbound = [&](int n) { return (double)n * lz - lgamma((double)n + 1.0); };
+    int lo = max(1, (int)ceil(z)), hi = nmax;
+    if (lo < hi && lbound(hi) < -700.0) {
+      while (lo < hi) {  // smallest n in [lo, hi] with bound < e^-700
+        const int mid = (lo + hi) >> 1;
+        if (lbound(mid) < -700.0) hi = mid;
+        else lo = mid + 1;
+      }
+      neff = lo;
+    }
+  }
+  for (int i = neff + 1; i <= nmax; ++i) row[i] = 0.0;
+  nmax = neff;
   int M = nmax;
   if ((double)M < z) M = (int)ceil(z);
   const int N = miller_start(M);
