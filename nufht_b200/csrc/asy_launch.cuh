@@ -18,7 +18,8 @@ AsyShape asy_shape(int NLP, int B, int LPT) {
   AsyShape L;
   L.LPT = LPT;
   L.NG = NLP / LPT;
-  int cap = std::max(1, std::min(256 / L.NG, 32));
+  // columns per CTA: up to 32, a multiple of 4 (16-byte pieces of the packed coefficients)
+  int cap = std::max(4, std::min(256 / L.NG, 32) & ~3);
   L.BT = std::min(cap, B);
   L.threads = L.BT * L.NG;
   L.V_total = NLP * B;
@@ -26,44 +27,32 @@ AsyShape asy_shape(int NLP, int B, int LPT) {
   return L;
 }
 
-template <typename T, int W, int LPT, bool WINDOWED, bool DIRECT>
-int launch_spread_kind(DevicePlan& D, const AsyClass& K, int item0, int nitems, const double* cs, int ld_cs,
-                       int B, cudaStream_t st) {
+template <typename T, int W, int LPT, bool TILE>
+int launch_spread_kind(DevicePlan& D, const AsyClass& K, int item0, int nitems, int B, cudaStream_t st) {
   if (nitems == 0) return 0;
+  using C2 = typename Cplx<T>::type;
   const AsyShape L = asy_shape(K.ac.NLP, B, LPT);
-  size_t sm = spread_smem<T>(W, L.BT * K.ac.NLP, L.NG, L.BT, WINDOWED && !DIRECT, K.ac.tile_cells).total;
+  const size_t sm = spread_smem<T>(W, K.ac.NLP, spread_btp<T>(L.BT)).total;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(k_asy_spread<T, W, LPT, WINDOWED, DIRECT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         220 * 1024);
+    cudaFuncSetAttribute(k_asy_spread<T, W, LPT, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     attr_set = true;
   }
   dim3 g((unsigned)nitems, (unsigned)L.ngy);
-  k_asy_spread<T, W, LPT, WINDOWED, DIRECT><<<g, L.threads, sm, st>>>(
-      D.d_rs, cs, ld_cs, B, (typename Cplx<T>::type*)D.d_grid, D.d_asyb, D.d_spread + item0, D.d_corr, K.ac,
-      L.BT, L.V_total);
+  k_asy_spread<T, W, LPT, TILE><<<g, L.threads, sm, st>>>(
+      static_cast<const T*>(D.d_ct), D.ldct, B, static_cast<C2*>(D.d_grid), D.d_asyb, D.d_spread + item0,
+      D.d_rec_l0, static_cast<const C2*>(D.d_rec_w), static_cast<const T*>(D.d_rec_p), K.ac.NLP, L.BT, L.V_total);
   NUFHT_LAUNCH_CHECK();
   return 0;
 }
 
-// Tiles store finished cells straight to the grid (each CTA owns its cells, so no atomics)
-// rather than through a shared window written out at the end: without the window more CTAs
-// fit on an SM, and L2 merges the scattered 8- or 16-byte stores of consecutive cells.
-// NUFHT_B200_SPREAD_DIRECT=0 selects the window form.
-inline bool spread_direct() {
-  static const bool on = [] {
-    const char* e = std::getenv("NUFHT_B200_SPREAD_DIRECT");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
-
+// Tiles (and the zero padding) own their cells; the source chunks of dense boxes add theirs
+// atomically.
 template <typename T, int W, int LPT>
-int launch_spread_lpt(DevicePlan& D, const AsyClass& K, const double* cs, int ld_cs, int B, cudaStream_t st) {
-  int rc = spread_direct() ? launch_spread_kind<T, W, LPT, true, true>(D, K, K.spread0, K.nspread, cs, ld_cs, B, st)
-                           : launch_spread_kind<T, W, LPT, true, false>(D, K, K.spread0, K.nspread, cs, ld_cs, B, st);
+int launch_spread_lpt(DevicePlan& D, const AsyClass& K, int B, cudaStream_t st) {
+  int rc = launch_spread_kind<T, W, LPT, true>(D, K, K.spread0, K.nspread, B, st);
   if (rc) return rc;
-  return launch_spread_kind<T, W, LPT, false, false>(D, K, K.spreadA0, K.nspreadA, cs, ld_cs, B, st);
+  return launch_spread_kind<T, W, LPT, false>(D, K, K.spreadA0, K.nspreadA, B, st);
 }
 
 template <typename T, int W, int LPT>
@@ -96,11 +85,34 @@ inline int lpt_small() {
   return v;
 }
 
+template <typename T>
+int build_records_t(DevicePlan& D) {
+  using C2 = typename Cplx<T>::type;
+  if (D.asyb.empty()) return 0;
+  const size_t b0 = sizeof(int) * (size_t)D.total_rec, b1 = sizeof(C2) * (size_t)D.total_recw,
+               b2 = sizeof(T) * (size_t)D.total_recp;
+  NUFHT_CUDA_TRY(cudaMalloc((void**)&D.d_rec_l0, b0));
+  NUFHT_CUDA_TRY(cudaMalloc(&D.d_rec_w, b1));
+  NUFHT_CUDA_TRY(cudaMalloc(&D.d_rec_p, b2));
+  D.rec_bytes = b0 + b1 + b2;
+  for (size_t q0 = 0; q0 < D.asyb.size();) {
+    size_t q1 = q0;
+    while (q1 < D.asyb.size() && D.asyb[q1].cls == D.asyb[q0].cls && q1 - q0 < 65535) ++q1;
+    const AsyClass& K = D.classes[D.asyb[q0].cls];
+    k_asy_records<T><<<dim3(64, (unsigned)(q1 - q0)), 256>>>(D.d_rs, D.d_asyb + q0, K.ac, K.W, D.d_corr,
+                                                              D.d_rec_l0, static_cast<C2*>(D.d_rec_w),
+                                                              static_cast<T*>(D.d_rec_p));
+    NUFHT_LAUNCH_CHECK();
+    q0 = q1;
+  }
+  return 0;
+}
+
 template <typename T, int W>
-int launch_spread(DevicePlan& D, const AsyClass& K, const double* cs, int ld_cs, int B, cudaStream_t st) {
-  if constexpr (sizeof(T) == 8 && W > 10) return launch_spread_lpt<T, W, 1>(D, K, cs, ld_cs, B, st);
-  else if (K.ac.NLP <= 4 && lpt_small() == 1) return launch_spread_lpt<T, W, 1>(D, K, cs, ld_cs, B, st);
-  else return launch_spread_lpt<T, W, 2>(D, K, cs, ld_cs, B, st);
+int launch_spread(DevicePlan& D, const AsyClass& K, int B, cudaStream_t st) {
+  if constexpr (sizeof(T) == 8 && W > 10) return launch_spread_lpt<T, W, 1>(D, K, B, st);
+  else if (K.ac.NLP <= 4 && lpt_small() == 1) return launch_spread_lpt<T, W, 1>(D, K, B, st);
+  else return launch_spread_lpt<T, W, 2>(D, K, B, st);
 }
 
 
@@ -142,6 +154,11 @@ int run_asy_t(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs,
     if (D.chunk_cell_end > D.chunk_cell_begin)
       NUFHT_CUDA_TRY(cudaMemsetAsync(grid + (size_t)D.chunk_cell_begin * B, 0,
                                      sizeof(C2) * (size_t)(D.chunk_cell_end - D.chunk_cell_begin) * B, st));
+    {  // coefficients source-major in the arithmetic type
+      dim3 g((unsigned)((D.m + 31) / 32), (unsigned)((D.ldct + 31) / 32));
+      k_pack_coefficients<T><<<g, dim3(32, 8), 0, st>>>(cs, ld_cs, B, D.m, static_cast<T*>(D.d_ct), D.ldct);
+      NUFHT_LAUNCH_CHECK();
+    }
     // the classes' boxes own disjoint grid ranges: their launches run concurrently
     int used[DevicePlan::kAuxStreams];
     int nu = 0;
@@ -157,7 +174,7 @@ int run_asy_t(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs,
     for (const AsyClass& K : D.classes) {
       if (K.nspread + K.nspreadA == 0) continue;
       cudaStream_t cs_st = D.serial ? st : D.aux[used[q++ % nu]];
-      NUFHT_W_DISPATCH(launch_spread, T, K.W, D, K, cs, ld_cs, B, cs_st);
+      NUFHT_W_DISPATCH(launch_spread, T, K.W, D, K, B, cs_st);
       if (rc) return rc;
     }
     if ((rc = join_streams(D, st, used, nu))) return rc;

@@ -501,11 +501,17 @@ void DevicePlan::build_lists() {
       }
       return a;
     };
-    const int TC = spread_tile_cells(d.nlp);
+    // A box is dense when one of its tiles (the layout of the work items below) would have
+    // more than kTileMaxSources sources.
+    const int TC = kSpreadTile;
     int worst = 0;
-    for (long long l = -half; l <= half; l += TC)
-      worst = std::max(worst, first_ge(l + TC + 1) - first_ge(l - Wb));
-    d.mode = (long long)worst * kSpreadTile > (long long)kTileMaxSources * TC ? 1 : 0;
+    for (long long l = 0; l <= half; l += TC)
+      worst = std::max(worst, first_ge(l + std::min<long long>(TC, half - l + 1)) - first_ge(l - Wb + 1));
+    for (long long l = -1; l >= -half; l -= TC) {
+      const long long lo = std::max(l - TC + 1, -half);
+      worst = std::max(worst, first_ge(l + 1) - first_ge(lo - Wb + 1));
+    }
+    d.mode = worst > kTileMaxSources ? 1 : 0;
     tmp.push_back(d);
   }
   // Layout: groups of consecutive boxes with equal (mode, n2, terms), mode-1 groups first so
@@ -518,6 +524,7 @@ void DevicePlan::build_lists() {
     return tmp[a].n2 < tmp[b].n2;
   });
   long long row = 0, coff = 0, poff = 0;
+  long long roff = 0, rwoff = 0, rpoff = 0;
   chunk_cell_begin = chunk_cell_end = 0;
   for (size_t q = 0; q < order.size();) {
     size_t e = q;
@@ -539,6 +546,15 @@ void DevicePlan::build_lists() {
       coff += 2LL * d.half + 1;
       poff += d.i1 - d.i0 + 1;
       row += (long long)d.n2 * d.nlp;
+      // source records: first cells, W weights and nlp factors per source (factor rows of a
+      // box start on a multiple of 4 values, for vector loads)
+      const long long nj = d.j1 - d.j0 + 1;
+      d.rec_off = roff;
+      d.recw_off = rwoff;
+      d.recp_off = rpoff;
+      roff += nj;
+      rwoff += nj * Wc[d.cls / kNlpClasses];
+      rpoff += (nj * d.nlp + 3) / 4 * 4;
       asyb.push_back(d);
     }
     if (gr.mode == 1) chunk_cell_end = row;
@@ -548,6 +564,9 @@ void DevicePlan::build_lists() {
   total_cells = row;
   total_corr = coff;
   total_post = poff;
+  total_rec = roff;
+  total_recw = rwoff;
+  total_recp = rpoff;
   // Work items, grouped by kernel class: windowed spreading items (mode 0 tiles and mode 2
   // zero padding), then atomic ones (mode 1 chunks of dense boxes).
   std::vector<SpreadItem> atomic_items;
@@ -600,7 +619,7 @@ void DevicePlan::build_lists() {
           s.je = first_ge((long long)l_start + ncell);
           spread.push_back(s);
         };
-        const int TC = spread_tile_cells(d.nlp);
+        const int TC = kSpreadTile;
         for (int l = 0; l <= d.half; l += TC) add_tile(l, std::min(TC, d.half - l + 1), l);
         for (int l = -1; l >= -d.half; l -= TC) {
           int lo = std::max(l - TC + 1, -d.half);
@@ -641,7 +660,6 @@ void DevicePlan::build_lists() {
     K.ninterp = (int)interp.size() - K.interp0;
     if (any) {
       K.ac = make_asy_const(P, K.nlp, K.W, es_beta(K.sigma, K.W));
-      K.ac.tile_cells = spread_tile_cells(K.nlp);
     }
     else std::memset(&K.ac, 0, sizeof(K.ac));
     classes.push_back(K);
@@ -691,6 +709,8 @@ int DevicePlan::upload_all() {
       NUFHT_LAUNCH_CHECK();
       b0 = b1;
     }
+    const int rc2 = mixed_asy ? asy_records_f32(*this) : asy_records_f64(*this);
+    if (rc2) return rc2;
     NUFHT_CUDA_TRY(cudaDeviceSynchronize());
   }
   return 0;
@@ -732,6 +752,7 @@ DevicePlan::~DevicePlan() {
   cudaFree(d_rs); cudaFree(d_ws); cudaFree(d_locb); cudaFree(d_proj); cudaFree(d_eval);
   cudaFree(d_dir); cudaFree(d_asyb); cudaFree(d_spread); cudaFree(d_interp);
   cudaFree(d_corr); cudaFree(d_post); cudaFree(d_jtab);
+  cudaFree(d_rec_l0); cudaFree(d_rec_w); cudaFree(d_rec_p); cudaFree(d_ct);
   cudaFree(d_grid); cudaFree(d_partial); cudaFree(d_cheb); cudaFree(d_fft_work);
   for (void* p : retired) cudaFree(p);
   cudaFree(d_stage_c); cudaFree(d_stage_g); cudaFree(d_stage_t);
@@ -835,14 +856,18 @@ int join_streams(DevicePlan& D, cudaStream_t st, const int* which, int n) {
 
 int DevicePlan::ensure_workspace(int B) {
   if (B <= ws_B) return ensure_fft(B);
-  drop_buffer(d_grid); drop_buffer(d_partial); drop_buffer(d_cheb);
-  d_grid = nullptr; d_partial = nullptr; d_cheb = nullptr;
+  drop_buffer(d_grid); drop_buffer(d_partial); drop_buffer(d_cheb); drop_buffer(d_ct);
+  d_grid = nullptr; d_partial = nullptr; d_cheb = nullptr; d_ct = nullptr;
   ws_B = 0;
   size_t bytes = 0;
   if (!asyb.empty()) {
     size_t g = (size_t)total_cells * (size_t)B * (mixed_asy ? sizeof(float2) : sizeof(double2));
     NUFHT_CUDA_TRY(cudaMalloc((void**)&d_grid, g));
     bytes += g;
+    ldct = packed_ld(B);
+    const size_t c = (size_t)m * (size_t)ldct * (mixed_asy ? sizeof(float) : sizeof(double));
+    NUFHT_CUDA_TRY(cudaMalloc(&d_ct, c));
+    bytes += c;
   }
   if (!locb.empty()) {
     size_t p = (size_t)proj.size() * KL1 * B * sizeof(double);

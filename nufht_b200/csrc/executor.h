@@ -44,6 +44,9 @@ struct AsyBoxD {
   long long cell_off;   // workspace offset in cells of one vector
   long long corr_off;   // first of 2 half + 1 entries in the cell table
   long long post_off;   // first of i1 - i0 + 1 entries in the target table
+  long long rec_off;    // source records of the box (sources j0..j1): first cells from rec_off,
+  long long recw_off;   // W weights each from recw_off,
+  long long recp_off;   // nlp amplitude factors each from recp_off
 };
 // Spreading work item.  mode 0: cells [l_start, l_start+ncell) of the box, FFT index
 // fft_start.., sources [js, je) whose support meets them; mode 1: all taps of sources
@@ -61,7 +64,6 @@ struct FftGroup {
 
 struct AsyConst {
   int NLP;      // 2 (K + 1)
-  int tile_cells;  // cells of a mode-0 spreading tile of this class
   int nq;       // quadrature nodes
   double beta;  // kernel shape
   double cos_phi, sin_phi;  // exp(i pi (-nu/2 - 1/4))
@@ -132,6 +134,7 @@ struct DevicePlan {
   long long chunk_cell_begin = 0;  // grid rows of the mode-1 boxes (zeroed before spreading)
   long long chunk_cell_end = 0;
   long long total_corr = 0, total_post = 0;
+  long long total_rec = 0, total_recw = 0, total_recp = 0;  // source record counts
   int NLP = 0;                     // 2 (K_asy + 1)
 
   // device copies
@@ -147,6 +150,12 @@ struct DevicePlan {
   int jtab_n = 0;             // unit intervals of d_jtab: it covers [0, jtab_n)
   double* d_corr = nullptr;   // 1 / psi-hat of the second stage, per box cell
   double2* d_post = nullptr;  // exp(i (phi + k C)) / psi-hat(theta_k), per box target
+  // Source records of the asymptotic boxes (arithmetic type of the boxes): first cell of
+  // each source's kernel support, its complex weights and its amplitude factors.
+  int* d_rec_l0 = nullptr;
+  void* d_rec_w = nullptr;
+  void* d_rec_p = nullptr;
+  size_t rec_bytes = 0;
 
   // workspace, sized for the largest batch executed so far
   int ws_B = 0;
@@ -160,6 +169,8 @@ struct DevicePlan {
   std::vector<void*> retired;
   size_t ws_bytes = 0;
   void* d_grid = nullptr;    // complex FP64 (double2) or, in mixed precision, FP32 (float2)
+  void* d_ct = nullptr;      // coefficients source-major, in the asymptotic boxes' type
+  int ldct = 0;              // row length of d_ct (columns, padded)
   bool mixed_asy = false;    // asymptotic boxes in FP32 (NUFHT_B200_MIXED, where FP32 meets tol)
   bool mixed_averaged = false;  // FP32 regardless of the worst-case bound (NUFHT_B200_MIXED_AVERAGED)
   double fp32_err = 0.0;     // modelled worst-case FP32 error of the asymptotic boxes per ||c||_1
@@ -239,6 +250,12 @@ int run_asy_f32(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_g
                 double sgn);
 int run_asy_f64(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
                 double sgn);
+// Source records of the asymptotic boxes (after the cell tables), in single or double precision.
+int asy_records_f32(DevicePlan& D);
+int asy_records_f64(DevicePlan& D);
+// Row length of the packed coefficients for batch size B: whole column blocks of a spreading
+// CTA (up to 32 columns) in 16-byte pieces.
+inline int packed_ld(int B) { return B <= 32 ? (B + 3) / 4 * 4 : (B + 31) / 32 * 32; }
 
 int run_besselj(double nu, const double* x, double* out, long count, cudaStream_t st);
 

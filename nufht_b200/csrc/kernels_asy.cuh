@@ -29,11 +29,11 @@
 
 namespace hankel {
 
-constexpr int kSpreadTile = 16;     // cells owned by one mode-0 spreading CTA at 8 or more terms
+constexpr int kSpreadTile = 32;     // cells owned by one mode-0 spreading CTA
 constexpr int kMinFft = 32;         // smallest FFT length of a box
 constexpr int kSpreadChunk = 64;    // sources staged in shared memory per round
 constexpr int kChunkSources = 2048; // sources per mode-1 work item, at most
-constexpr int kTileMaxSources = 4096;
+constexpr int kTileMaxSources = 2048;  // sources of a mode-0 tile, at most (denser boxes: mode 1)
 constexpr int kInterpTile = 128;    // targets per interpolation CTA
 constexpr int kInterpChunk = 32;    // targets per shared-memory round
 
@@ -59,26 +59,11 @@ __device__ __forceinline__ float es_kernel_t(float u, float ihw, float beta) {
 
 // Work split of the spreading and interpolation CTAs.  Thread (tl, g) owns LPT
 // consecutive expansion terms lp = g LPT .. g LPT + LPT - 1 of column t0 + tl, so every
-// kernel weight read from shared memory feeds 2 LPT multiply-adds (register blocking), and
-// the LPT source amplitudes (rref / r)^(lp + 1/2) c follow from one staged value by
-// multiplications with rref / r.  NG = NLP / LPT threads per column, BT columns per CTA.
+// kernel weight read from shared memory feeds 2 LPT multiply-adds (register blocking).
+// NG = NLP / LPT threads per column, BT columns per CTA.
 struct AsyShape {
   int LPT, NG, BT, threads, ngy, V_total;
 };
-
-// Cells of a mode-0 spreading tile (AsyConst::tile_cells, chosen per kernel class at plan
-// time): 16 at 6 or more expansion terms, 32 at 2 or 4 (whose CTAs have one term per thread,
-// NLP / 1 threads per column), or NUFHT_B200_TILE_CELLS_SMALL for 2 and 4 terms.  A window
-// (cells x (vectors + 1) complex values, when tiles write through shared memory) of these
-// sizes stays near 16 KB for 2 and 4 terms and 33 KB for 8.
-inline int spread_tile_cells(int nlp) {
-  static const int small = [] {
-    const char* e = std::getenv("NUFHT_B200_TILE_CELLS_SMALL");
-    const int v = e ? std::atoi(e) : 0;
-    return (v >= 8 && v <= 256) ? v : 2 * kSpreadTile;
-  }();
-  return nlp >= 6 ? kSpreadTile : small;
-}
 
 // Staged kernel weights per source (complex) and per target (real), padded so that every
 // row is read with 16-byte shared-memory loads.
@@ -89,26 +74,43 @@ __host__ __device__ constexpr int interp_we(int W) { return sizeof(T) == 4 ? (W 
 
 __host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
-// Shared-memory layout of k_asy_spread (byte offsets, each region 16-byte aligned); the
-// host sizes the launch with the same function.
+// Shared-memory layout of k_asy_spread: two buffers (the chunk being walked and the next one,
+// filled by asynchronous copies), each with the chunk's first cells, run ends, weights (rows
+// of WE complex values), amplitude factors (rows of NLP) and coefficients (rows of BTP
+// columns); byte offsets, each region 16-byte aligned.  The host sizes the launch with the
+// same function.
 struct SpreadSmem {
-  size_t win, wc, rq, c, u, ph, l0, end, total;
+  size_t l0, end, w, p, c, buf, total;
 };
 template <typename T>
-__host__ __device__ inline SpreadSmem spread_smem(int W, int VCTA, int NG, int BT, bool windowed, int tile_cells) {
+__host__ __device__ inline SpreadSmem spread_smem(int W, int NLP, int BTP) {
   SpreadSmem L{};
   const size_t c2 = 2 * sizeof(T);
-  L.win = 0;
-  L.wc = align16(L.win + (windowed ? (size_t)tile_cells * (VCTA + 1) * c2 : 0));
-  L.rq = align16(L.wc + (size_t)kSpreadChunk * spread_we<T>(W) * c2);
-  L.c = align16(L.rq + (size_t)kSpreadChunk * NG * c2);
-  L.u = align16(L.c + (size_t)BT * (kSpreadChunk + 1) * sizeof(T));
-  L.ph = align16(L.u + (size_t)kSpreadChunk * sizeof(double));
-  L.l0 = align16(L.ph + (size_t)kSpreadChunk * c2);
+  L.l0 = 0;
   L.end = align16(L.l0 + (size_t)kSpreadChunk * 4);
-  L.total = align16(L.end + (size_t)kSpreadChunk * 4);
+  L.w = align16(L.end + (size_t)kSpreadChunk * 4);
+  L.p = align16(L.w + (size_t)kSpreadChunk * spread_we<T>(W) * c2);
+  L.c = align16(L.p + (size_t)kSpreadChunk * NLP * sizeof(T));
+  L.buf = align16(L.c + (size_t)kSpreadChunk * BTP * sizeof(T));
+  L.total = 2 * L.buf;
   return L;
 }
+// Coefficient row of a spreading CTA in shared memory: BT columns rounded up to 16 bytes.
+template <typename T>
+__host__ __device__ constexpr int spread_btp(int BT) { return sizeof(T) == 4 ? (BT + 3) & ~3 : (BT + 1) & ~1; }
+
+// Asynchronous global -> shared copies (cp.async, completed by cp_async_wait_all).
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // Index one past the run of equal values that contains a[s] in the non-decreasing a[0, n).
 __device__ __forceinline__ int run_end(const int* a, int n, int s) {
@@ -219,43 +221,100 @@ __device__ __forceinline__ void grid_atomic_add(double2* p, double2 v) {
   atomicAdd(&p->y, v.y);
 }
 
-// Stage 1.  Sources are sorted, so the first cell l0 of their kernel support never
-// decreases.  The CTA walks the cells c in order; at cell c it adds every source with
-// l0 == c into W register accumulators per vector, then cell c is final and leaves.  The
-// accumulators form a ring indexed (position + tap) mod W, and the walk is unrolled W times
-// so that every ring index is a compile-time constant: no register moves as the window
-// advances.  A finished cell goes to a shared window of the CTA's own cells (WINDOWED,
-// mode-0 tiles; written to the grid with coalesced stores at the end) or is added
-// atomically to the pre-zeroed grid (mode-1 source chunks of dense boxes).  Empty stretches
-// between sources are skipped once the ring is empty.  The source phase exp(i D x) is folded
-// into complex kernel weights staged once per source.
-template <typename T, int W, int LPT, bool WINDOWED, bool DIRECT = false>
+// Plan-time source records of stage 1 (k_asy_spread), per box and source j: first cell of
+// the kernel support at rec_off + (j - j0), W complex weights at recw_off + (j - j0) W and NLP
+// amplitude factors at recp_off + (j - j0) NLP.  The weights and the first cell follow from
+// the same FP64 position u = (r - C) / h as the cell tables; the weights are rounded to the
+// arithmetic type after the kernel value (evaluated in that type), the deconvolution factor
+// and the source phase are applied.
+template <typename T>
+__global__ void k_asy_records(const double* __restrict__ rs, const AsyBoxD* __restrict__ boxes, AsyConst P, int W,
+                              const double* __restrict__ corr, int* __restrict__ rl0,
+                              typename Cplx<T>::type* __restrict__ rw, T* __restrict__ rp) {
+  const AsyBoxD bx = boxes[blockIdx.y];
+  const int nj = bx.j1 - bx.j0 + 1;
+  const T ihw = (T)(2.0 / (double)W);
+  const T beta = (T)P.beta;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nj; q += gridDim.x * blockDim.x) {
+    const double r = rs[bx.j0 + q];
+    const double x = r - bx.C;
+    const double u = x / bx.h;
+    const int l0 = (int)ceil(u - 0.5 * W);
+    rl0[bx.rec_off + q] = l0;
+    double sn, cn;
+    sincos(bx.D * x, &sn, &cn);
+    const T phx = (T)cn, phy = (T)sn;
+    for (int e = 0; e < W; ++e) {
+      const int cell = l0 + e;
+      const T w = (cell >= -bx.half && cell <= bx.half)
+                      ? es_kernel_t((T)((double)cell - u), ihw, beta) * (T)corr[bx.corr_off + cell + bx.half]
+                      : (T)0;
+      rw[bx.recw_off + (long long)q * W + e] = cmake<T>(w * phx, w * phy);
+    }
+    const double ir = r > 0.0 ? bx.rref / r : 0.0;  // sources at r = 0 contribute nothing
+    double pw = sqrt(ir);
+    for (int lp = 0; lp < bx.nlp; ++lp, pw *= ir) rp[bx.recp_off + (long long)q * bx.nlp + lp] = (T)pw;
+  }
+}
+
+// ct[j * ldct + t] = cs[t * ld_cs + j] in the arithmetic type (zero for t >= B): 32 x 32
+// tiles through shared memory, coalesced on both sides.
+template <typename T>
+__global__ void __launch_bounds__(256) k_pack_coefficients(const double* __restrict__ cs, int ld_cs, int B, int m,
+                                                           T* __restrict__ ct, int ldct) {
+  __shared__ double tile[32][33];
+  const int j0 = blockIdx.x * 32, t0 = blockIdx.y * 32;
+  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+    const int t = t0 + ty, j = j0 + threadIdx.x;
+    tile[ty][threadIdx.x] = (t < B && j < m) ? cs[(size_t)t * ld_cs + j] : 0.0;
+  }
+  __syncthreads();
+  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+    const int j = j0 + ty, t = t0 + threadIdx.x;
+    if (j < m && t < ldct) ct[(size_t)j * ldct + t] = (T)tile[threadIdx.x][ty];
+  }
+}
+
+// Stage 1.  Everything about a source except its coefficients is fixed when the plan is
+// made, so the plan keeps, per (box, source) pair (k_asy_records): the first cell l0 of its
+// kernel support, its W complex weights psi(l0 + q - u) exp(i D x) / psi-hat(l0 + q) (zero
+// outside [-half, half]) and its NLP amplitude factors (rref / r)^(lp + 1/2).  A transform packs
+// its coefficients source-major in the arithmetic type (k_pack_coefficients), and a spreading
+// CTA copies its sources' records and coefficients to shared memory in chunks of kSpreadChunk
+// with cp.async, the next chunk in flight while the current one is walked.
+//
+// Sources are sorted, so l0 never decreases.  The CTA walks the cells in order; at cell c it
+// adds every source with l0 == c into W register accumulators per vector, then cell c is final
+// and leaves.  The accumulators form a ring indexed (position + tap) mod W, and the walk is
+// unrolled W times so that every ring index is a compile-time constant: no register moves as
+// the window advances.  TILE items (mode 0) own their cells and store each one exactly once,
+// zeros where no source reaches; the source chunks of dense boxes (mode 1) add their cells
+// atomically to the pre-zeroed grid.  Empty stretches between sources are skipped once the
+// ring is empty.
+template <typename T, int W, int LPT, bool TILE>
 __global__ void __launch_bounds__(256) k_asy_spread(
-    const double* __restrict__ rs, const double* __restrict__ cs, int ld_cs, int B,
-    typename Cplx<T>::type* __restrict__ grid, const AsyBoxD* __restrict__ boxes,
-    const SpreadItem* __restrict__ items, const double* __restrict__ corr, AsyConst P, int BT,
-    int V_total) {
+    const T* __restrict__ ct, int ldct, int B, typename Cplx<T>::type* __restrict__ grid,
+    const AsyBoxD* __restrict__ boxes, const SpreadItem* __restrict__ items, const int* __restrict__ rl0,
+    const typename Cplx<T>::type* __restrict__ rw, const T* __restrict__ rp, int NLP, int BT, int V_total) {
   using C2 = typename Cplx<T>::type;
-  constexpr int SCP = kSpreadChunk + 1;  // padded row of the staged coefficients
   constexpr int WE = spread_we<T>(W);
+  constexpr int PER16 = 16 / (int)sizeof(T);  // values per 16-byte copy
   const SpreadItem it = items[blockIdx.x];
   const AsyBoxD bx = boxes[it.box];
-  const int NLP = P.NLP;
   const int NG = NLP / LPT;
   const int nthr = blockDim.x;
   const int VCTA = BT * NLP;
-  const int WP = VCTA + 1;  // padded window row
   const int tid = threadIdx.x;
   const int tl = tid / NG, g = tid - tl * NG;
   const int t0 = blockIdx.y * BT;
   const int v0 = t0 * NLP;
-  const int nv = min(VCTA, V_total - v0);  // valid vectors of this CTA
-  const int vloc = tl * NLP + g * LPT;     // first of this thread's vectors within the CTA
+  const int vloc = tl * NLP + g * LPT;  // first of this thread's vectors within the CTA
   const bool active = tl < BT && t0 + tl < B;
   C2* gbox = grid + (size_t)bx.cell_off * (size_t)B;
   const int nc = it.ncell;
 
-  if (WINDOWED && it.mode == 2) {  // zero padding of the FFT input: threads along cells
+  if (TILE && it.mode == 2) {  // zero padding of the FFT input: threads along cells
+    const int nv = min(VCTA, V_total - v0);
     for (int e = tid; e < nc * nv; e += nthr) {
       int vv = e / nc, cell = e - vv * nc;
       gbox[(size_t)(v0 + vv) * bx.n2 + it.fft_start + cell] = cmake<T>(0, 0);
@@ -264,60 +323,54 @@ __global__ void __launch_bounds__(256) k_asy_spread(
   }
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int TC = P.tile_cells;
-  const SpreadSmem L = spread_smem<T>(W, VCTA, NG, BT, WINDOWED && !DIRECT, TC);
-  C2* win = reinterpret_cast<C2*>(smem_raw + L.win);        // [TC][WP]
-  C2* s_wc = reinterpret_cast<C2*>(smem_raw + L.wc);        // [SCH][WE]
-  C2* s_rq = reinterpret_cast<C2*>(smem_raw + L.rq);        // [SCH][NG]: (rho of term g LPT, rref / r)
-  T* s_c = reinterpret_cast<T*>(smem_raw + L.c);            // [BT][SCP]
-  double* s_u = reinterpret_cast<double*>(smem_raw + L.u);  // [SCH]
-  C2* s_ph = reinterpret_cast<C2*>(smem_raw + L.ph);        // [SCH]: exp(i D x)
-  int* s_l0 = reinterpret_cast<int*>(smem_raw + L.l0);      // [SCH]
-  int* s_end = reinterpret_cast<int*>(smem_raw + L.end);    // [SCH]: end of the equal-l0 run
+  const int BTP = spread_btp<T>(BT);
+  const SpreadSmem L = spread_smem<T>(W, NLP, BTP);
+  const int nsrc = it.je - it.js;
+  const int jr0 = it.js - bx.j0;  // first source of the item within its box
 
-  if (WINDOWED && !DIRECT)
-    for (int e = tid; e < TC * WP; e += nthr) win[e] = cmake<T>(0, 0);
-  const T ihw = (T)(2.0 / (double)W);
-  const T beta = (T)P.beta;
-
-  // Stage sources [s0, s0 + ns) (all threads; barriers on both sides).
-  auto stage = [&](int s0, int ns) {
-    __syncthreads();  // previous round fully consumed
-    for (int s = tid; s < ns; s += nthr) {
-      double r = rs[s0 + s];
-      double x = r - bx.C;
-      double u = x / bx.h;
-      s_u[s] = u;
-      s_l0[s] = (int)ceil(u - 0.5 * W);
-      double sn, cn;
-      sincos(bx.D * x, &sn, &cn);
-      s_ph[s] = cmake<T>((T)cn, (T)sn);
-      double ir = r > 0.0 ? bx.rref / r : 0.0;  // sources at r = 0 contribute nothing
-      double rho = sqrt(ir);
-      for (int q = 0; q < NG; ++q) {
-        s_rq[s * NG + q] = cmake<T>((T)rho, (T)ir);
-        for (int z = 0; z < LPT; ++z) rho *= ir;
-      }
+  // Copies of the item's sources [s0, s0 + ns) into buffer b (one commit group).
+  auto issue = [&](int b, int s0, int ns) {
+    unsigned char* base = smem_raw + (size_t)b * L.buf;
+    int* d_l0 = reinterpret_cast<int*>(base + L.l0);
+    C2* d_w = reinterpret_cast<C2*>(base + L.w);
+    T* d_p = reinterpret_cast<T*>(base + L.p);
+    T* d_c = reinterpret_cast<T*>(base + L.c);
+    const int js = jr0 + s0;
+    for (int s = tid; s < ns; s += nthr) cp_async4(d_l0 + s, rl0 + bx.rec_off + js + s);
+    const C2* gw = rw + bx.recw_off + (long long)js * W;
+    for (int e = tid; e < ns * W; e += nthr) {
+      const int s = e / W, q = e - s * W;
+      if constexpr (sizeof(T) == 4) cp_async8(d_w + s * WE + q, gw + e);
+      else cp_async16(d_w + s * WE + q, gw + e);
     }
-    for (int e = tid; e < ns * BT; e += nthr) {
-      int tt = e / ns, s = e - tt * ns;
-      s_c[tt * SCP + s] = (T)((t0 + tt < B) ? cs[(size_t)(t0 + tt) * ld_cs + s0 + s] : 0.0);
+    // factors in pairs (NLP is even and the rows of a box start on a multiple of 4 values)
+    const T* gp = rp + bx.recp_off + (long long)js * NLP;
+    for (int e = tid; e < ns * NLP / 2; e += nthr) {
+      if constexpr (sizeof(T) == 4) cp_async8(d_p + 2 * e, gp + 2 * e);
+      else cp_async16(d_p + 2 * e, gp + 2 * e);
     }
-    __syncthreads();
-    // complex weights psi(l - u) exp(i D x) / psi-hat(cell l): the deconvolution factor of the
-    // target cell is folded in here (loaded in parallel with the other weights), so finished
-    // cells are stored as they are
-    for (int e = tid; e < ns * WE; e += nthr) {
-      int s = e / WE, q = e - s * WE;
-      const int cell = s_l0[s] + q;
-      T w = (q < W && cell >= -bx.half && cell <= bx.half)
-                ? es_kernel_t((T)((double)cell - s_u[s]), ihw, beta) * (T)corr[bx.corr_off + cell + bx.half]
-                : (T)0;
-      C2 ph = s_ph[s];
-      s_wc[e] = cmake<T>(w * ph.x, w * ph.y);
+    // coefficients: BTP columns per source in 16-byte pieces (ldct and t0 are multiples of 4;
+    // pieces past the packed row are columns >= B, whose threads store nothing)
+    const int npc = BTP / PER16;
+    const T* gc = ct + (size_t)(it.js + s0) * ldct + t0;
+    for (int e = tid; e < ns * npc; e += nthr) {
+      const int s = e / npc, q = e - s * npc;
+      if (t0 + q * PER16 < ldct) cp_async16(d_c + s * BTP + q * PER16, gc + (size_t)s * ldct + q * PER16);
     }
-    for (int s = tid; s < ns; s += nthr) s_end[s] = run_end(s_l0, ns, s);
-    __syncthreads();
+    cp_async_commit();
+  };
+  const int* s_l0 = nullptr;
+  int* s_end = nullptr;
+  const C2* s_w = nullptr;
+  const T* s_p = nullptr;
+  const T* s_c = nullptr;
+  auto point = [&](int b) {
+    unsigned char* base = smem_raw + (size_t)b * L.buf;
+    s_l0 = reinterpret_cast<const int*>(base + L.l0);
+    s_end = reinterpret_cast<int*>(base + L.end);
+    s_w = reinterpret_cast<const C2*>(base + L.w);
+    s_p = reinterpret_cast<const T*>(base + L.p);
+    s_c = reinterpret_cast<const T*>(base + L.c);
   };
 
   C2 acc[LPT][W];
@@ -326,11 +379,11 @@ __global__ void __launch_bounds__(256) k_asy_spread(
 #pragma unroll
     for (int q = 0; q < W; ++q) acc[u][q] = cmake<T>(0, 0);
 
-  // DIRECT tiles write every cell they own exactly once, in increasing order: cells the walk
-  // skips (no source support) get zeros.  zc = first owned cell not written yet.
+  // Tiles write every cell they own exactly once, in increasing order: cells the walk skips
+  // (no source support) get zeros.  zc = first owned cell not written yet.
   int zc = it.l_start;
   auto zero_to = [&](int upto) {  // zeros for owned cells [zc, upto)
-    if (!(WINDOWED && DIRECT)) return;
+    if (!TILE) return;
     const int hi = min(upto, it.l_start + nc);
     if (active)
       for (int cc = max(zc, it.l_start); cc < hi; ++cc) {
@@ -341,19 +394,22 @@ __global__ void __launch_bounds__(256) k_asy_spread(
     zc = max(zc, hi);
   };
 
-  if (it.je > it.js) {
-    int s0 = it.js;
-    int ns = min(kSpreadChunk, it.je - s0);
-    stage(s0, ns);
+  if (nsrc > 0) {
+    int s0 = 0;  // item-relative first source of the current chunk
+    int ns = min(kSpreadChunk, nsrc);
+    int cur = 0;
+    issue(0, 0, ns);
+    if (ns < nsrc) issue(1, ns, min(kSpreadChunk, nsrc - ns));
+    cp_async_wait_all();
+    __syncthreads();
+    point(0);
+    for (int s = tid; s < ns; s += nthr) s_end[s] = run_end(s_l0, ns, s);
+    __syncthreads();
     int sp = 0;
     int c = s_l0[0];
     // last cell to visit: the last source's support end, or the tile's end
-    int c_end;
-    {
-      double ul = (rs[it.je - 1] - bx.C) / bx.h;
-      c_end = (int)ceil(ul - 0.5 * W) + W - 1;
-      if (WINDOWED) c_end = min(c_end, it.l_start + nc - 1);
-    }
+    int c_end = rl0[bx.rec_off + jr0 + nsrc - 1] + W - 1;
+    if (TILE) c_end = min(c_end, it.l_start + nc - 1);
     int last = INT_MIN / 2;  // cell of the latest source added
     bool done = c > c_end;
     while (!done) {
@@ -362,20 +418,27 @@ __global__ void __launch_bounds__(256) k_asy_spread(
         // sources whose support starts at cell c (ring position jj)
         for (;;) {
           if (sp < ns && s_l0[sp] == c) {
-            // the run of sources with l0 == c in this chunk: a known trip count, two
-            // sources per step so that the shared loads of both issue together
             const int e = s_end[sp];
             if (tl < BT) {
               auto add = [&](int s) {
-                const C2 rq = s_rq[s * NG + g];
-                T a = s_c[tl * SCP + s] * rq.x;
+                const T cv = s_c[s * BTP + tl];
                 C2 wc[WE];
-                load_weights<WE>(s_wc + s * WE, wc);
+                load_weights<WE>(s_w + s * WE, wc);
+                T pv[LPT];
+                if constexpr (LPT == 2) {
+                  const typename Cplx<T>::type pp =
+                      *reinterpret_cast<const typename Cplx<T>::type*>(s_p + s * NLP + g * LPT);
+                  pv[0] = pp.x;
+                  pv[LPT - 1] = pp.y;
+                } else {
+#pragma unroll
+                  for (int u = 0; u < LPT; ++u) pv[u] = s_p[s * NLP + g * LPT + u];
+                }
 #pragma unroll
                 for (int u = 0; u < LPT; ++u) {
+                  const T a = cv * pv[u];
 #pragma unroll
                   for (int q = 0; q < W; ++q) cfma(acc[u][(jj + q) % W], wc[q], a);
-                  a *= rq.y;
                 }
               };
 #pragma unroll 1
@@ -384,29 +447,31 @@ __global__ void __launch_bounds__(256) k_asy_spread(
             last = c;
             sp = e;
           }
-          if (sp < ns || s0 + ns >= it.je) break;
+          if (sp < ns || s0 + ns >= nsrc) break;
+          // the next chunk (already in flight) becomes current; the buffer just released
+          // takes the one after it
+          cp_async_wait_all();
+          __syncthreads();
+          cur ^= 1;
           s0 += ns;
-          ns = min(kSpreadChunk, it.je - s0);
-          stage(s0, ns);
+          ns = min(kSpreadChunk, nsrc - s0);
+          point(cur);
+          for (int s = tid; s < ns; s += nthr) s_end[s] = run_end(s_l0, ns, s);
+          if (s0 + ns < nsrc) issue(cur ^ 1, s0 + ns, min(kSpreadChunk, nsrc - s0 - ns));
+          __syncthreads();
           sp = 0;
         }
         // cell c is final
         if (active) {
-          if (WINDOWED) {
+          if (TILE) {
             const int cl = c - it.l_start;
             if (cl >= 0 && cl < nc) {
-              if (DIRECT) {
-                // the CTA owns the cell: zeros for the owned cells skipped before it, then
-                // the cell scaled by 1/psi-hat, for each vector
-                zero_to(c);
-                zc = c + 1;
-                const int idx = it.fft_start + cl;
+              // the CTA owns the cell: zeros for the owned cells skipped before it, then the cell
+              zero_to(c);
+              zc = c + 1;
+              const int idx = it.fft_start + cl;
 #pragma unroll
-                for (int u = 0; u < LPT; ++u) gbox[(size_t)(v0 + vloc + u) * bx.n2 + idx] = acc[u][jj];
-              } else {
-#pragma unroll
-                for (int u = 0; u < LPT; ++u) win[cl * WP + vloc + u] = acc[u][jj];
-              }
+              for (int u = 0; u < LPT; ++u) gbox[(size_t)(v0 + vloc + u) * bx.n2 + idx] = acc[u][jj];
             }
           } else if (c >= -bx.half && c <= bx.half) {
             const int idx = c < 0 ? c + bx.n2 : c;
@@ -432,14 +497,6 @@ __global__ void __launch_bounds__(256) k_asy_spread(
     }
   }
   zero_to(INT_MAX);  // owned cells after the walk (or all of them when no source reaches the tile)
-  if (!WINDOWED || DIRECT) return;
-  __syncthreads();
-  // Transposed write-out of the CTA's own cells: consecutive threads take consecutive
-  // cells of one vector.
-  for (int e = tid; e < nc * nv; e += nthr) {
-    int vv = e / nc, cell = e - vv * nc;
-    gbox[(size_t)(v0 + vv) * bx.n2 + it.fft_start + cell] = win[cell * WP + vv];
-  }
 }
 
 // Stage 3.  Thread (tl, g) owns terms g LPT .. g LPT + LPT - 1 of column t0 + tl.  Targets
