@@ -66,9 +66,10 @@ int launch_interp_lpt(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, i
     attr_set = true;
   }
   dim3 g((unsigned)K.ninterp, (unsigned)L.ngy);
-  k_asy_interp<T, W, LPT><<<g, L.threads, sm, st>>>(D.d_ws, gs, ld_gs, B, (const typename Cplx<T>::type*)D.d_grid,
-                                                    D.d_asyb, D.d_interp + K.interp0, D.d_post, K.ac, L.BT,
-                                                    L.V_total, sgn);
+  using C2 = typename Cplx<T>::type;
+  k_asy_interp<T, W, LPT><<<g, L.threads, sm, st>>>(gs, ld_gs, B, static_cast<const C2*>(D.d_grid), D.d_asyb,
+                                                    D.d_interp + K.interp0, D.d_tq0, static_cast<const T*>(D.d_tw),
+                                                    static_cast<const C2*>(D.d_tmu), K.ac.NLP, L.BT, sgn);
   NUFHT_LAUNCH_CHECK();
   return 0;
 }
@@ -91,10 +92,15 @@ int build_records_t(DevicePlan& D) {
   if (D.asyb.empty()) return 0;
   const size_t b0 = sizeof(int) * (size_t)D.total_rec, b1 = sizeof(C2) * (size_t)D.total_recw,
                b2 = sizeof(T) * (size_t)D.total_recp;
+  const size_t b3 = sizeof(int) * (size_t)D.total_post, b4 = sizeof(T) * (size_t)D.total_tw,
+               b5 = sizeof(C2) * (size_t)D.total_tm;
   NUFHT_CUDA_TRY(cudaMalloc((void**)&D.d_rec_l0, b0));
   NUFHT_CUDA_TRY(cudaMalloc(&D.d_rec_w, b1));
   NUFHT_CUDA_TRY(cudaMalloc(&D.d_rec_p, b2));
-  D.rec_bytes = b0 + b1 + b2;
+  NUFHT_CUDA_TRY(cudaMalloc((void**)&D.d_tq0, b3));
+  NUFHT_CUDA_TRY(cudaMalloc(&D.d_tw, b4));
+  NUFHT_CUDA_TRY(cudaMalloc(&D.d_tmu, b5));
+  D.rec_bytes = b0 + b1 + b2 + b3 + b4 + b5;
   for (size_t q0 = 0; q0 < D.asyb.size();) {
     size_t q1 = q0;
     while (q1 < D.asyb.size() && D.asyb[q1].cls == D.asyb[q0].cls && q1 - q0 < 65535) ++q1;
@@ -102,6 +108,10 @@ int build_records_t(DevicePlan& D) {
     k_asy_records<T><<<dim3(64, (unsigned)(q1 - q0)), 256>>>(D.d_rs, D.d_asyb + q0, K.ac, K.W, D.d_corr,
                                                               D.d_rec_l0, static_cast<C2*>(D.d_rec_w),
                                                               static_cast<T*>(D.d_rec_p));
+    NUFHT_LAUNCH_CHECK();
+    k_asy_target_records<T><<<dim3(64, (unsigned)(q1 - q0)), 256>>>(D.d_ws, D.d_asyb + q0, K.ac, K.W, D.d_tq0,
+                                                                     static_cast<T*>(D.d_tw),
+                                                                     static_cast<C2*>(D.d_tmu));
     NUFHT_LAUNCH_CHECK();
     q0 = q1;
   }

@@ -524,7 +524,7 @@ void DevicePlan::build_lists() {
     return tmp[a].n2 < tmp[b].n2;
   });
   long long row = 0, coff = 0, poff = 0;
-  long long roff = 0, rwoff = 0, rpoff = 0;
+  long long roff = 0, rwoff = 0, rpoff = 0, twoff = 0, tmoff = 0;
   chunk_cell_begin = chunk_cell_end = 0;
   for (size_t q = 0; q < order.size();) {
     size_t e = q;
@@ -544,7 +544,12 @@ void DevicePlan::build_lists() {
       d.corr_off = coff;
       d.post_off = poff;
       coff += 2LL * d.half + 1;
-      poff += d.i1 - d.i0 + 1;
+      const long long ni = d.i1 - d.i0 + 1;
+      d.tw_off = twoff;
+      d.tm_off = tmoff;
+      poff += ni;
+      twoff += ni * (mixed_asy ? interp_we<float>(Wc[d.cls / kNlpClasses]) : interp_we<double>(Wc[d.cls / kNlpClasses]));
+      tmoff += ni * d.nlp;
       row += (long long)d.n2 * d.nlp;
       // source records: first cells, W weights and nlp factors per source (factor rows of a
       // box start on a multiple of 4 values, for vector loads)
@@ -567,6 +572,8 @@ void DevicePlan::build_lists() {
   total_rec = roff;
   total_recw = rwoff;
   total_recp = rpoff;
+  total_tw = twoff;
+  total_tm = tmoff;
   // Work items, grouped by kernel class: windowed spreading items (mode 0 tiles and mode 2
   // zero padding), then atomic ones (mode 1 chunks of dense boxes).
   std::vector<SpreadItem> atomic_items;
@@ -696,7 +703,6 @@ int DevicePlan::upload_all() {
   if (!asyb.empty()) {
     if (NLP > kMaxNLP) return NUFHT_E_TOO_LARGE;
     NUFHT_CUDA_TRY(cudaMalloc((void**)&d_corr, sizeof(double) * (size_t)total_corr));
-    NUFHT_CUDA_TRY(cudaMalloc((void**)&d_post, sizeof(double2) * (size_t)total_post));
     // Tables per box with the constants of the box's kernel class.
     for (size_t b0 = 0; b0 < asyb.size();) {
       size_t b1 = b0;
@@ -704,8 +710,6 @@ int DevicePlan::upload_all() {
       const AsyConst& A = classes[asyb[b0].cls].ac;
       unsigned cnt = (unsigned)(b1 - b0);
       k_asy_setup_cells<<<dim3(64, cnt), 256>>>(d_asyb + b0, A, d_corr);
-      NUFHT_LAUNCH_CHECK();
-      k_asy_setup_targets<<<dim3(64, cnt), 256>>>(d_ws, d_asyb + b0, A, d_post);
       NUFHT_LAUNCH_CHECK();
       b0 = b1;
     }
@@ -751,8 +755,9 @@ DevicePlan::~DevicePlan() {
   release_fft();
   cudaFree(d_rs); cudaFree(d_ws); cudaFree(d_locb); cudaFree(d_proj); cudaFree(d_eval);
   cudaFree(d_dir); cudaFree(d_asyb); cudaFree(d_spread); cudaFree(d_interp);
-  cudaFree(d_corr); cudaFree(d_post); cudaFree(d_jtab);
+  cudaFree(d_corr); cudaFree(d_jtab);
   cudaFree(d_rec_l0); cudaFree(d_rec_w); cudaFree(d_rec_p); cudaFree(d_ct);
+  cudaFree(d_tq0); cudaFree(d_tw); cudaFree(d_tmu);
   cudaFree(d_grid); cudaFree(d_partial); cudaFree(d_cheb); cudaFree(d_fft_work);
   for (void* p : retired) cudaFree(p);
   cudaFree(d_stage_c); cudaFree(d_stage_g); cudaFree(d_stage_t);

@@ -43,7 +43,9 @@ struct AsyBoxD {
   int nlp;              // expansion terms of this box: 2 (K + 1) with K <= K_asy
   long long cell_off;   // workspace offset in cells of one vector
   long long corr_off;   // first of 2 half + 1 entries in the cell table
-  long long post_off;   // first of i1 - i0 + 1 entries in the target table
+  long long post_off;   // target records of the box (targets i0..i1): first cells from post_off,
+  long long tw_off;     // interpolation weights (rows padded to 16 bytes) from tw_off,
+  long long tm_off;     // nlp target factors each from tm_off
   long long rec_off;    // source records of the box (sources j0..j1): first cells from rec_off,
   long long recw_off;   // W weights each from recw_off,
   long long recp_off;   // nlp amplitude factors each from recp_off
@@ -135,6 +137,7 @@ struct DevicePlan {
   long long chunk_cell_end = 0;
   long long total_corr = 0, total_post = 0;
   long long total_rec = 0, total_recw = 0, total_recp = 0;  // source record counts
+  long long total_tw = 0, total_tm = 0;                      // target record counts
   int NLP = 0;                     // 2 (K_asy + 1)
 
   // device copies
@@ -149,12 +152,16 @@ struct DevicePlan {
   double* d_jtab = nullptr;   // J_nu table of the direct boxes (orders whose evaluation is costly)
   int jtab_n = 0;             // unit intervals of d_jtab: it covers [0, jtab_n)
   double* d_corr = nullptr;   // 1 / psi-hat of the second stage, per box cell
-  double2* d_post = nullptr;  // exp(i (phi + k C)) / psi-hat(theta_k), per box target
   // Source records of the asymptotic boxes (arithmetic type of the boxes): first cell of
   // each source's kernel support, its complex weights and its amplitude factors.
   int* d_rec_l0 = nullptr;
   void* d_rec_w = nullptr;
   void* d_rec_p = nullptr;
+  // Target records: first cell of each target's stencil, its W kernel weights and its NLP
+  // factors mu (expansion coefficient, target power, phase and deconvolution).
+  int* d_tq0 = nullptr;
+  void* d_tw = nullptr;
+  void* d_tmu = nullptr;
   size_t rec_bytes = 0;
 
   // workspace, sized for the largest batch executed so far

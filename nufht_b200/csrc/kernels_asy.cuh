@@ -124,25 +124,27 @@ __device__ __forceinline__ int run_end(const int* a, int n, int s) {
   return lo;
 }
 
-// Shared-memory layout of k_asy_interp.
+// Shared-memory layout of k_asy_interp: the per-thread partial sums of a chunk of targets,
+// then two buffers (the chunk being walked and the next one, filled by asynchronous copies of
+// the target records), each with the chunk's factors mu, weights, first cells and run ends.
 struct InterpSmem {
-  size_t mu, y, wt, q0, end, uu, total;
+  size_t y, buf0, mu, wt, q0, end, buf, total;
 };
 template <typename T>
 __host__ __device__ inline InterpSmem interp_smem(int W, int NLP, int threads) {
   InterpSmem L{};
+  L.y = 0;
+  L.buf0 = align16((size_t)kInterpChunk * (threads + 1) * sizeof(T));
   L.mu = 0;
-  L.y = align16(L.mu + (size_t)kInterpChunk * NLP * 2 * sizeof(T));
-  L.wt = align16(L.y + (size_t)kInterpChunk * (threads + 1) * sizeof(T));
+  L.wt = align16(L.mu + (size_t)kInterpChunk * NLP * 2 * sizeof(T));
   L.q0 = align16(L.wt + (size_t)kInterpChunk * interp_we<T>(W) * sizeof(T));
   L.end = align16(L.q0 + (size_t)kInterpChunk * 4);
-  L.uu = align16(L.end + (size_t)kInterpChunk * 4);
-  L.total = align16(L.uu + (size_t)kInterpChunk * sizeof(double));
+  L.buf = align16(L.end + (size_t)kInterpChunk * 4);
+  L.total = L.buf0 + 2 * L.buf;
   return L;
 }
 
-// Plan-time tables: 1/psi-hat(2 pi l / n2) for each box cell l, and
-// exp(i (phi + k C)) / psi-hat((k - D) h) for each box target.
+// Plan-time table: 1/psi-hat(2 pi l / n2) for each box cell l.
 static __global__ void k_asy_setup_cells(const AsyBoxD* __restrict__ boxes, AsyConst P,
                                   double* __restrict__ corr) {
   const AsyBoxD bx = boxes[blockIdx.y];
@@ -152,17 +154,41 @@ static __global__ void k_asy_setup_cells(const AsyBoxD* __restrict__ boxes, AsyC
   }
 }
 
-static __global__ void k_asy_setup_targets(const double* __restrict__ ws, const AsyBoxD* __restrict__ boxes,
-                                    AsyConst P, double2* __restrict__ post) {
+// Plan-time target records of stage 3 (k_asy_interp), per box and target i: the first cell
+// q0 of its stencil at post_off + (i - i0), its W kernel weights at tw_off + (i - i0) WE
+// (zeros after W), and its NLP factors
+//   mu_lp = coef_lp (k rref)^-(lp + 1/2) exp(i (phi + k C)) / psi-hat((k - D) h)
+// (rotated by i for odd lp) at tm_off + (i - i0) NLP, computed in FP64 and rounded to the
+// arithmetic type; the weights are evaluated in that type at the FP64 offset u - (q0 + e).
+template <typename T>
+__global__ void k_asy_target_records(const double* __restrict__ ws, const AsyBoxD* __restrict__ boxes, AsyConst P,
+                                     int W, int* __restrict__ tq0, T* __restrict__ tw,
+                                     typename Cplx<T>::type* __restrict__ tmu) {
   const AsyBoxD bx = boxes[blockIdx.y];
   const int ni = bx.i1 - bx.i0 + 1;
+  const int WE = interp_we<T>(W);
+  const T ihw = (T)(2.0 / (double)W);
+  const T beta = (T)P.beta;
+  const double u_scale = bx.h * (double)bx.n2 / (2.0 * M_PI);
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ni; q += gridDim.x * blockDim.x) {
-    double k = ws[bx.i0 + q];
-    double inv_hat = 1.0 / es_hat(P, (k - bx.D) * bx.h);
+    const double k = ws[bx.i0 + q];
+    const double uu = (k - bx.D) * u_scale;
+    const int q0 = (int)ceil(uu - 0.5 * W);
+    tq0[bx.post_off + q] = q0;
+    for (int e = 0; e < WE; ++e)
+      tw[bx.tw_off + (long long)q * WE + e] = e < W ? es_kernel_t((T)(uu - (double)(q0 + e)), ihw, beta) : (T)0;
+    const double inv_hat = 1.0 / es_hat(P, (k - bx.D) * bx.h);
     double sn, cn;
     sincos(k * bx.C, &sn, &cn);
-    double er = cn * P.cos_phi - sn * P.sin_phi, ei = sn * P.cos_phi + cn * P.sin_phi;
-    post[bx.post_off + q] = make_double2(er * inv_hat, ei * inv_hat);
+    const double psx = (cn * P.cos_phi - sn * P.sin_phi) * inv_hat;
+    const double psy = (sn * P.cos_phi + cn * P.sin_phi) * inv_hat;
+    const double ik = 1.0 / (k * bx.rref);
+    double pw = sqrt(ik);
+    for (int lp = 0; lp < bx.nlp; ++lp, pw *= ik) {
+      const double sc = P.coef[lp] * pw;
+      const double mr = sc * psx, mi = sc * psy;
+      tmu[bx.tm_off + (long long)q * bx.nlp + lp] = (lp & 1) ? cmake<T>((T)-mi, (T)mr) : cmake<T>((T)mr, (T)mi);
+    }
   }
 }
 
@@ -499,27 +525,27 @@ __global__ void __launch_bounds__(256) k_asy_spread(
   zero_to(INT_MAX);  // owned cells after the walk (or all of them when no source reaches the tile)
 }
 
-// Stage 3.  Thread (tl, g) owns terms g LPT .. g LPT + LPT - 1 of column t0 + tl.  Targets
-// are sorted, so the first cell q0 of their stencil never decreases; the CTA walks the cells
-// in order with a ring of R = W + 1 grid values per vector in registers (the stencil plus one
-// cell fetched a step ahead); the walk is unrolled R times, which makes every ring index a
-// compile-time constant.  Each thread combines its terms with the per-target factors mu
-// (rounded to the arithmetic type from their FP64 values) and leaves its partial sum in
-// shared memory; at the end of each chunk of targets the NG partials of a column are added
-// in FP64 and atomically into g, consecutive threads taking consecutive targets of a column.
-// (Warp shuffles for the partial sums measured slower on B200.)
+// Stage 3.  Thread (tl, g) owns terms g LPT .. g LPT + LPT - 1 of column t0 + tl.  The target
+// records (k_asy_target_records) are copied to shared memory in chunks of kInterpChunk with
+// cp.async, the next chunk in flight while the current one is walked.  Targets are sorted, so
+// the first cell q0 of their stencil never decreases; the CTA walks the cells in order with a
+// ring of R = W + 1 grid values per vector in registers (the stencil plus one cell fetched a
+// step ahead); the walk is unrolled R times, which makes every ring index a compile-time
+// constant.  Each thread combines its terms with the per-target factors mu and leaves its
+// partial sum in shared memory; at the end of each chunk of targets the NG partials of a
+// column are added in FP64 and atomically into g, consecutive threads taking consecutive
+// targets of a column.  (Warp shuffles for the partial sums measured slower on B200.)
 template <typename T, int W, int LPT>
 __global__ void __launch_bounds__(256) k_asy_interp(
-    const double* __restrict__ ws, double* __restrict__ gs, int ld_gs, int B,
-    const typename Cplx<T>::type* __restrict__ grid, const AsyBoxD* __restrict__ boxes,
-    const InterpItem* __restrict__ items, const double2* __restrict__ post, AsyConst P, int BT,
-    int V_total, double sgn) {
+    double* __restrict__ gs, int ld_gs, int B, const typename Cplx<T>::type* __restrict__ grid,
+    const AsyBoxD* __restrict__ boxes, const InterpItem* __restrict__ items, const int* __restrict__ tq0,
+    const T* __restrict__ tw, const typename Cplx<T>::type* __restrict__ tmu, int NLP, int BT, double sgn) {
   using C2 = typename Cplx<T>::type;
   constexpr int WE = interp_we<T>(W);
   constexpr int R = W + 1;
+  constexpr int PER16 = 16 / (int)sizeof(T);  // values per 16-byte copy
   const InterpItem it = items[blockIdx.x];
   const AsyBoxD bx = boxes[it.box];
-  const int NLP = P.NLP;
   const int NG = NLP / LPT;
   const int nthr = blockDim.x;
   const int YP = nthr + 1;  // padded row of the per-target partial sums
@@ -530,12 +556,35 @@ __global__ void __launch_bounds__(256) k_asy_interp(
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const InterpSmem L = interp_smem<T>(W, NLP, nthr);
-  C2* s_mu = reinterpret_cast<C2*>(smem_raw + L.mu);        // [KC][NLP]
   T* s_y = reinterpret_cast<T*>(smem_raw + L.y);  // [KC][YP]: per-thread partial sums (already in T)
-  T* s_wt = reinterpret_cast<T*>(smem_raw + L.wt);          // [KC][WE]
-  int* s_q0 = reinterpret_cast<int*>(smem_raw + L.q0);      // [KC]
-  int* s_end = reinterpret_cast<int*>(smem_raw + L.end);    // [KC]: end of the equal-q0 run
-  double* s_uu = reinterpret_cast<double*>(smem_raw + L.uu);  // [KC]: target position in cells
+  const C2* s_mu = nullptr;  // [KC][NLP]
+  const T* s_wt = nullptr;   // [KC][WE]
+  const int* s_q0 = nullptr; // [KC]
+  int* s_end = nullptr;      // [KC]: end of the equal-q0 run
+  auto point = [&](int b) {
+    unsigned char* base = smem_raw + L.buf0 + (size_t)b * L.buf;
+    s_mu = reinterpret_cast<const C2*>(base + L.mu);
+    s_wt = reinterpret_cast<const T*>(base + L.wt);
+    s_q0 = reinterpret_cast<const int*>(base + L.q0);
+    s_end = reinterpret_cast<int*>(base + L.end);
+  };
+  // Copies of the records of targets [k0, k0 + nk) into buffer b (one commit group).
+  auto issue = [&](int b, int k0, int nk) {
+    unsigned char* base = smem_raw + L.buf0 + (size_t)b * L.buf;
+    C2* d_mu = reinterpret_cast<C2*>(base + L.mu);
+    T* d_wt = reinterpret_cast<T*>(base + L.wt);
+    int* d_q0 = reinterpret_cast<int*>(base + L.q0);
+    const int q = k0 - bx.i0;
+    for (int kk = tid; kk < nk; kk += nthr) cp_async4(d_q0 + kk, tq0 + bx.post_off + q + kk);
+    const T* gw = tw + bx.tw_off + (long long)q * WE;  // rows of WE values: 16-byte pieces
+    for (int e = tid; e < nk * WE / PER16; e += nthr) cp_async16(d_wt + e * PER16, gw + e * PER16);
+    const C2* gm = tmu + bx.tm_off + (long long)q * NLP;
+    for (int e = tid; e < nk * NLP; e += nthr) {
+      if constexpr (sizeof(T) == 4) cp_async8(d_mu + e, gm + e);
+      else cp_async16(d_mu + e, gm + e);
+    }
+    cp_async_commit();
+  };
 
   const int n2 = bx.n2;
   const C2* row[LPT];
@@ -543,45 +592,12 @@ __global__ void __launch_bounds__(256) k_asy_interp(
   for (int u = 0; u < LPT; ++u)
     row[u] = grid + (size_t)bx.cell_off * (size_t)B +
              (size_t)(active ? (t0 + tl) * NLP + g * LPT + u : 0) * (size_t)n2;
-  const T ihw = (T)(2.0 / (double)W);
-  const T beta = (T)P.beta;
-  const double u_scale = bx.h * (double)n2 / (2.0 * M_PI);
 
   auto fetch = [&](int cell, int u) -> C2 {
     int idx = cell < 0 ? cell + n2 : (cell >= n2 ? cell - n2 : cell);
     return active ? row[u][idx] : cmake<T>(0, 0);
   };
 
-  // Stage targets [k0, k0 + nk) (all threads; barriers on both sides).
-  auto stage = [&](int k0, int nk) {
-    __syncthreads();
-    // per target (one thread each): stencil start, and the NLP factors
-    // mu_q = coef_q (k rref)^{-(q + 1/2)} exp(i (phi + k C)) / psi-hat, rotated by i for odd q,
-    // with one square root and one reciprocal per target
-    for (int kk = tid; kk < nk; kk += nthr) {
-      const double k = ws[k0 + kk];
-      const double uu = (k - bx.D) * u_scale;
-      s_uu[kk] = uu;
-      s_q0[kk] = (int)ceil(uu - 0.5 * W);
-      const double2 ps = post[bx.post_off + (k0 + kk - bx.i0)];
-      const double kr = k * bx.rref;
-      const double ik = 1.0 / kr;
-      double pw = sqrt(ik);
-      for (int q = 0; q < NLP; ++q, pw *= ik) {
-        const double sc = P.coef[q] * pw;
-        const double mr = sc * ps.x, mi = sc * ps.y;
-        s_mu[kk * NLP + q] = (q & 1) ? cmake<T>((T)-mi, (T)mr) : cmake<T>((T)mr, (T)mi);
-      }
-    }
-    __syncthreads();
-    // kernel weights over all (target, tap) pairs
-    for (int e = tid; e < nk * WE; e += nthr) {
-      const int kk = e / WE, q = e - kk * WE;
-      s_wt[e] = q < W ? es_kernel_t((T)(s_uu[kk] - (double)(s_q0[kk] + q)), ihw, beta) : (T)0;
-    }
-    for (int kk = tid; kk < nk; kk += nthr) s_end[kk] = run_end(s_q0, nk, kk);
-    __syncthreads();
-  };
   // Sum the NG partials of each column and add them to g (all threads).
   auto flush = [&](int k0, int nk) {
     __syncthreads();
@@ -598,7 +614,14 @@ __global__ void __launch_bounds__(256) k_asy_interp(
   if (it.ke <= it.ks) return;
   int k0 = it.ks;
   int nk = min(kInterpChunk, it.ke - k0);
-  stage(k0, nk);
+  int cur = 0;
+  issue(0, k0, nk);
+  if (k0 + nk < it.ke) issue(1, k0 + nk, min(kInterpChunk, it.ke - k0 - nk));
+  cp_async_wait_all();
+  __syncthreads();
+  point(0);
+  for (int kk = tid; kk < nk; kk += nthr) s_end[kk] = run_end(s_q0, nk, kk);
+  __syncthreads();
   int kp = 0;
   int c = s_q0[0];
   C2 gw[LPT][R];
@@ -640,9 +663,17 @@ __global__ void __launch_bounds__(256) k_asy_interp(
           done = true;
           break;
         }
+        // the next chunk (already in flight) becomes current; the buffer just released takes
+        // the one after it
+        cp_async_wait_all();
+        __syncthreads();  // partial sums read, current buffer released, copies visible
+        cur ^= 1;
         k0 += nk;
         nk = min(kInterpChunk, it.ke - k0);
-        stage(k0, nk);
+        point(cur);
+        for (int kk = tid; kk < nk; kk += nthr) s_end[kk] = run_end(s_q0, nk, kk);
+        if (k0 + nk < it.ke) issue(cur ^ 1, k0 + nk, min(kInterpChunk, it.ke - k0 - nk));
+        __syncthreads();
         kp = 0;
       }
       if (done) break;
