@@ -493,16 +493,22 @@ def main():
 
     # Roofline of the dominant kernel (the phase with the largest device time).
     hbm, hbm_kind = peaks()
-    sf = np.zeros(12)
-    sa = np.zeros(12)
-    lib.nufht_b200_plan_stats(pf._h, sf.ctypes.data_as(L.c_double_p), 12)
-    lib.nufht_b200_plan_stats(pa._h, sa.ctypes.data_as(L.c_double_p), 12)
+    sf = np.zeros(21)
+    sa = np.zeros(21)
+    lib.nufht_b200_plan_stats(pf._h, sf.ctypes.data_as(L.c_double_p), 21)
+    lib.nufht_b200_plan_stats(pa._h, sa.ctypes.data_as(L.c_double_p), 21)
     V = sf[10] * B
     gb = 8.0 if mixed else 16.0  # bytes per complex grid value (FP32 / FP64)
-    byts = {  # algorithmic bytes per fwd+adj step (both plans)
-        "asy_spread": sum(8.0 * s[0] * (B + 1) + gb * s[2] * V for s in (sf, sa)),
+    ev = gb / 2  # bytes per value of the arithmetic type
+    # algorithmic bytes per fwd+adj step (both plans): spreading reads the source records and
+    # each box's packed coefficients and writes the grid (the packing pass reads c once and
+    # writes its packed copy); interpolation reads the grid cells its stencils reach and the
+    # target records, and adds one value per target and column into g
+    npts = {id(sf): N, id(sa): M}
+    byts = {
+        "asy_spread": sum(s[19] + ev * s[0] * B + gb * s[2] * V + (8.0 + ev) * npts[id(s)] * B for s in (sf, sa)),
         "asy_fft": sum(2 * gb * s[2] * V for s in (sf, sa)),
-        "asy_interp": sum(gb * s[8] * V + 8.0 * s[1] * (2 * B + 1) for s in (sf, sa)),
+        "asy_interp": sum(gb * s[8] * V + s[20] + 8.0 * s[1] * B for s in (sf, sa)),
     }
     flops = {
         "asy_spread": sum(4.0 * s[3] * V for s in (sf, sa)),

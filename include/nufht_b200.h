@@ -247,7 +247,8 @@ int nufht_b200_phase_times(double *ms, int nphase);
  * precision) else 0, and the modelled worst-case error of FP32 asymptotic boxes per unit
  * ||c||_1 (mixed precision is used only where it is at most tol / 4); out[15..17] the
  * planning time in ms (grid validation and box partition, work lists, device tables and
- * uploads) and out[18] 1 when the partition ran on the device. */
+ * uploads), out[18] 1 when the partition ran on the device, and out[19..20] the bytes of the
+ * plan-time source records (read by spreading) and target records (read by interpolation). */
 int nufht_b200_plan_stats(const NufhtDevicePlan *plan, double *out, int n);
 
 /* Measured FP64 fused-multiply-add throughput of the current device (TFLOP/s). */

@@ -27,12 +27,23 @@ AsyShape asy_shape(int NLP, int B, int LPT) {
   return L;
 }
 
+// Sources per shared-memory round of spreading (NUFHT_B200_SPREAD_CHUNK, 16..64, default 64).
+inline int spread_chunk() {
+  static const int v = [] {
+    const char* e = std::getenv("NUFHT_B200_SPREAD_CHUNK");
+    const int q = e ? std::atoi(e) : kSpreadChunk;
+    return (q >= 16 && q <= kSpreadChunk) ? q : kSpreadChunk;
+  }();
+  return v;
+}
+
 template <typename T, int W, int LPT, bool TILE>
 int launch_spread_kind(DevicePlan& D, const AsyClass& K, int item0, int nitems, int B, cudaStream_t st) {
   if (nitems == 0) return 0;
   using C2 = typename Cplx<T>::type;
   const AsyShape L = asy_shape(K.ac.NLP, B, LPT);
-  const size_t sm = spread_smem<T>(W, K.ac.NLP, spread_btp<T>(L.BT)).total;
+  const int sch = spread_chunk();
+  const size_t sm = spread_smem<T>(W, K.ac.NLP, spread_btp<T>(L.BT), sch).total;
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(k_asy_spread<T, W, LPT, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
@@ -41,7 +52,8 @@ int launch_spread_kind(DevicePlan& D, const AsyClass& K, int item0, int nitems, 
   dim3 g((unsigned)nitems, (unsigned)L.ngy);
   k_asy_spread<T, W, LPT, TILE><<<g, L.threads, sm, st>>>(
       static_cast<const T*>(D.d_ct), D.ldct, B, static_cast<C2*>(D.d_grid), D.d_asyb, D.d_spread + item0,
-      D.d_rec_l0, static_cast<const C2*>(D.d_rec_w), static_cast<const T*>(D.d_rec_p), K.ac.NLP, L.BT, L.V_total);
+      D.d_rec_l0, static_cast<const C2*>(D.d_rec_w), static_cast<const T*>(D.d_rec_p), K.ac.NLP, L.BT, L.V_total,
+      sch);
   NUFHT_LAUNCH_CHECK();
   return 0;
 }

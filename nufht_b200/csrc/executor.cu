@@ -44,6 +44,22 @@ const bool g_loc_simt = [] {
   return e && e[0] == '1';
 }();
 
+// Direct boxes on the tensor-core kernel (Bessel tiles in shared memory, DMMA products;
+// NUFHT_B200_DIR_MMA=1) instead of the SIMT one (one thread or a few lanes per target, the
+// multiply-adds on the FP64 pipe), which measured faster on B200 (direct phase 3.0 against 4.8
+// ms per step at the 1e6-point workload).
+const bool g_dir_simt = [] {
+  const char* e = std::getenv("NUFHT_B200_DIR_MMA");
+  return !(e && e[0] == '1');
+}();
+
+// Direct boxes evaluate J_nu directly instead of through the plan-time table
+// (NUFHT_B200_DIR_NO_TABLE=1).
+const bool g_dir_no_table = [] {
+  const char* e = std::getenv("NUFHT_B200_DIR_NO_TABLE");
+  return e && e[0] == '1';
+}();
+
 namespace {
 
 std::mutex g_phase_mu;
@@ -400,16 +416,33 @@ void DevicePlan::build_lists() {
   }
   std::vector<HBox> all_dir = dir_boxes;
   all_dir.insert(all_dir.end(), asy_direct.begin(), asy_direct.end());
-  for (const HBox& hb : all_dir) {
-    int ni = hb.i1 - hb.i0 + 1;
-    int lanes = ni >= kDirThreads ? 1 : std::min(32, kDirThreads / next_pow2(ni));
-    int tpc = kDirThreads / lanes;  // targets per CTA
-    // The same number of sources per item for every shape: thin boxes (few targets, many
-    // sources) split into many CTAs instead of a few long-running ones.
-    int spi = kDirSources;
-    for (int i = hb.i0; i <= hb.i1; i += tpc)
-      for (int j = hb.j0; j <= hb.j1; j += spi)
-        dir.push_back({i, std::min(tpc, hb.i1 - i + 1), j, std::min(spi, hb.j1 - j + 1), lanes});
+  dir_thin = 0;
+  dir_simt = g_dir_simt;
+  if (dir_simt) {
+    for (const HBox& hb : all_dir) {
+      int ni = hb.i1 - hb.i0 + 1;
+      int lanes = ni >= kDirThreads ? 1 : std::min(32, kDirThreads / next_pow2(ni));
+      int tpc = kDirThreads / lanes;  // targets per CTA
+      // The same number of sources per item for every shape: thin boxes (few targets, many
+      // sources) split into many CTAs instead of a few long-running ones.
+      int spi = kDirSources;
+      for (int i = hb.i0; i <= hb.i1; i += tpc)
+        for (int j = hb.j0; j <= hb.j1; j += spi)
+          dir.push_back({i, std::min(tpc, hb.i1 - i + 1), j, std::min(spi, hb.j1 - j + 1), lanes});
+    }
+  } else {
+    // Tensor-core items: blocks of up to 64 targets x kDirMmaSources sources; blocks of at most
+    // 16 targets take the thin tile shape and come first in the list.
+    std::vector<DirItem> wide;
+    for (const HBox& hb : all_dir)
+      for (int i = hb.i0; i <= hb.i1; i += 64) {
+        const int nb = std::min(64, hb.i1 - i + 1);
+        std::vector<DirItem>& to = nb <= 16 ? dir : wide;
+        for (int j = hb.j0; j <= hb.j1; j += kDirMmaSources)
+          to.push_back({i, nb, j, std::min(kDirMmaSources, hb.j1 - j + 1), 0});
+      }
+    dir_thin = (int)dir.size();
+    dir.insert(dir.end(), wide.begin(), wide.end());
   }
   // ---- asymptotic boxes
   asyb.clear();
@@ -689,9 +722,12 @@ int DevicePlan::upload_all() {
       (rc = upload(interp, &d_interp)))
     return rc;
   // J_nu table for the direct boxes where J_nu costs a recurrence over the order (integer
-  // orders from 2, half-integer orders from 3/2) and their arguments k r stay below the
-  // table's reach; larger arguments are evaluated directly.
-  if (!dir.empty() && nu2 >= 3) {
+  // orders from 2, half-integer orders from 3/2), for their arguments k r below the table's
+  // reach (larger arguments are evaluated directly).  Orders 0, 1 and 1/2 evaluate directly:
+  // there the table's 128 bytes per pair, a different line for each lane of a tall box,
+  // measured slower on B200 than the Chebyshev and Hankel forms (direct phase 2.97 against
+  // 3.22 ms per step at the 1e6-point workload).
+  if (!dir.empty() && nu2 >= 3 && !g_dir_no_table) {
     double xmax = 0.0;
     for (const DirItem& it : dir) xmax = std::max(xmax, h_ws[it.i0 + it.ni - 1] * h_rs[it.j0 + it.nj - 1]);
     jtab_n = (int)std::min<double>(std::ceil(xmax) + 1.0, (double)kJTabMaxIntervals);
@@ -905,6 +941,32 @@ int launch_dir(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs
   return 0;
 }
 
+template <int ROWS, int NTN>
+int launch_dir_mma_items(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B,
+                         cudaStream_t st, double sgn, int item0, int nitems) {
+  if (nitems <= 0) return 0;
+  const size_t sm = DirMmaSmem<ROWS>::bytes(8 * NTN);
+  static bool attr_set = false;
+  if (!attr_set) {
+    NUFHT_CUDA_TRY(cudaFuncSetAttribute(k_dir_mma<ROWS, NTN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    attr_set = true;
+  }
+  dim3 g((unsigned)nitems, (unsigned)((B + 8 * NTN - 1) / (8 * NTN)));
+  k_dir_mma<ROWS, NTN><<<g, 128, sm, st>>>(D.d_rs, D.d_ws, cs, ld_cs, gs, ld_gs, B, D.d_dir + item0, D.nu2, sgn,
+                                            D.d_jtab, D.jtab_n);
+  NUFHT_LAUNCH_CHECK();
+  return 0;
+}
+
+template <int NTN>
+int launch_dir_mma(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
+                   double sgn) {
+  int rc = launch_dir_mma_items<16, NTN>(D, cs, ld_cs, gs, ld_gs, B, st, sgn, 0, D.dir_thin);
+  if (rc) return rc;
+  return launch_dir_mma_items<64, NTN>(D, cs, ld_cs, gs, ld_gs, B, st, sgn, D.dir_thin,
+                                       (int)D.dir.size() - D.dir_thin);
+}
+
 // Shared-memory budget of the local-expansion kernels (doubles).
 constexpr size_t kLocSmemDoubles = 200 * 1024 / 8;
 
@@ -1082,7 +1144,12 @@ int DevicePlan::run(const double* cs, int ld_cs, double* gs, int ld_gs, int B, c
   }
   if (!dir.empty()) {
     PhaseScope ps(kPhaseDir, s_dir);
-    if (B >= 32) rc = launch_dir<32>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);
+    if (!dir_simt) {
+      if (B >= 25) rc = launch_dir_mma<4>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);
+      else if (B >= 17) rc = launch_dir_mma<3>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);
+      else if (B >= 9) rc = launch_dir_mma<2>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);
+      else rc = launch_dir_mma<1>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);
+    } else if (B >= 32) rc = launch_dir<32>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);
     else if (B >= 16) rc = launch_dir<16>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);
     else if (B >= 8) rc = launch_dir<8>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);
     else if (B >= 4) rc = launch_dir<4>(*this, cs, ld_cs, gs, ld_gs, B, s_dir, sgn);

@@ -126,7 +126,9 @@ struct DevicePlan {
   std::vector<LocBoxD> locb;
   std::vector<ProjItem> proj;
   std::vector<EvalItem> eval;
-  std::vector<DirItem> dir;
+  std::vector<DirItem> dir;       // direct items (tensor-core form: the dir_thin thin ones first)
+  int dir_thin = 0;
+  bool dir_simt = false;          // direct items of the SIMT kernel
   std::vector<AsyBoxD> asyb;
   std::vector<SpreadItem> spread;
   std::vector<InterpItem> interp;

@@ -31,7 +31,7 @@ namespace hankel {
 
 constexpr int kSpreadTile = 32;     // cells owned by one mode-0 spreading CTA
 constexpr int kMinFft = 32;         // smallest FFT length of a box
-constexpr int kSpreadChunk = 64;    // sources staged in shared memory per round
+constexpr int kSpreadChunk = 64;    // sources staged in shared memory per round, at most
 constexpr int kChunkSources = 2048; // sources per mode-1 work item, at most
 constexpr int kTileMaxSources = 2048;  // sources of a mode-0 tile, at most (denser boxes: mode 1)
 constexpr int kInterpTile = 128;    // targets per interpolation CTA
@@ -83,15 +83,15 @@ struct SpreadSmem {
   size_t l0, end, w, p, c, buf, total;
 };
 template <typename T>
-__host__ __device__ inline SpreadSmem spread_smem(int W, int NLP, int BTP) {
+__host__ __device__ inline SpreadSmem spread_smem(int W, int NLP, int BTP, int SCH) {
   SpreadSmem L{};
   const size_t c2 = 2 * sizeof(T);
   L.l0 = 0;
-  L.end = align16(L.l0 + (size_t)kSpreadChunk * 4);
-  L.w = align16(L.end + (size_t)kSpreadChunk * 4);
-  L.p = align16(L.w + (size_t)kSpreadChunk * spread_we<T>(W) * c2);
-  L.c = align16(L.p + (size_t)kSpreadChunk * NLP * sizeof(T));
-  L.buf = align16(L.c + (size_t)kSpreadChunk * BTP * sizeof(T));
+  L.end = align16(L.l0 + (size_t)SCH * 4);
+  L.w = align16(L.end + (size_t)SCH * 4);
+  L.p = align16(L.w + (size_t)SCH * spread_we<T>(W) * c2);
+  L.c = align16(L.p + (size_t)SCH * NLP * sizeof(T));
+  L.buf = align16(L.c + (size_t)SCH * BTP * sizeof(T));
   L.total = 2 * L.buf;
   return L;
 }
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(256) k_pack_coefficients(const double* __restr
 // kernel support, its W complex weights psi(l0 + q - u) exp(i D x) / psi-hat(l0 + q) (zero
 // outside [-half, half]) and its NLP amplitude factors (rref / r)^(lp + 1/2).  A transform packs
 // its coefficients source-major in the arithmetic type (k_pack_coefficients), and a spreading
-// CTA copies its sources' records and coefficients to shared memory in chunks of kSpreadChunk
+// CTA copies its sources' records and coefficients to shared memory in chunks of SCH sources
 // with cp.async, the next chunk in flight while the current one is walked.
 //
 // Sources are sorted, so l0 never decreases.  The CTA walks the cells in order; at cell c it
@@ -321,7 +321,8 @@ template <typename T, int W, int LPT, bool TILE>
 __global__ void __launch_bounds__(256) k_asy_spread(
     const T* __restrict__ ct, int ldct, int B, typename Cplx<T>::type* __restrict__ grid,
     const AsyBoxD* __restrict__ boxes, const SpreadItem* __restrict__ items, const int* __restrict__ rl0,
-    const typename Cplx<T>::type* __restrict__ rw, const T* __restrict__ rp, int NLP, int BT, int V_total) {
+    const typename Cplx<T>::type* __restrict__ rw, const T* __restrict__ rp, int NLP, int BT, int V_total,
+    int SCH) {
   using C2 = typename Cplx<T>::type;
   constexpr int WE = spread_we<T>(W);
   constexpr int PER16 = 16 / (int)sizeof(T);  // values per 16-byte copy
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(256) k_asy_spread(
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int BTP = spread_btp<T>(BT);
-  const SpreadSmem L = spread_smem<T>(W, NLP, BTP);
+  const SpreadSmem L = spread_smem<T>(W, NLP, BTP, SCH);
   const int nsrc = it.je - it.js;
   const int jr0 = it.js - bx.j0;  // first source of the item within its box
 
@@ -422,17 +423,20 @@ __global__ void __launch_bounds__(256) k_asy_spread(
 
   if (nsrc > 0) {
     int s0 = 0;  // item-relative first source of the current chunk
-    int ns = min(kSpreadChunk, nsrc);
+    int ns = min(SCH, nsrc);
     int cur = 0;
     issue(0, 0, ns);
-    if (ns < nsrc) issue(1, ns, min(kSpreadChunk, nsrc - ns));
+    if (ns < nsrc) issue(1, ns, min(SCH, nsrc - ns));
     cp_async_wait_all();
     __syncthreads();
     point(0);
     for (int s = tid; s < ns; s += nthr) s_end[s] = run_end(s_l0, ns, s);
     __syncthreads();
     int sp = 0;
-    int c = s_l0[0];
+    // first cell and run end of source sp, kept in registers (loaded when sp moves, so that
+    // the loads overlap the work before the next test)
+    int ln = s_l0[0], en = s_end[0];
+    int c = ln;
     // last cell to visit: the last source's support end, or the tile's end
     int c_end = rl0[bx.rec_off + jr0 + nsrc - 1] + W - 1;
     if (TILE) c_end = min(c_end, it.l_start + nc - 1);
@@ -443,8 +447,12 @@ __global__ void __launch_bounds__(256) k_asy_spread(
       for (int jj = 0; jj < W; ++jj) {
         // sources whose support starts at cell c (ring position jj)
         for (;;) {
-          if (sp < ns && s_l0[sp] == c) {
-            const int e = s_end[sp];
+          if (sp < ns && ln == c) {
+            const int e = en;
+            if (e < ns) {
+              ln = s_l0[e];
+              en = s_end[e];
+            }
             if (tl < BT) {
               auto add = [&](int s) {
                 const T cv = s_c[s * BTP + tl];
@@ -480,12 +488,14 @@ __global__ void __launch_bounds__(256) k_asy_spread(
           __syncthreads();
           cur ^= 1;
           s0 += ns;
-          ns = min(kSpreadChunk, nsrc - s0);
+          ns = min(SCH, nsrc - s0);
           point(cur);
           for (int s = tid; s < ns; s += nthr) s_end[s] = run_end(s_l0, ns, s);
-          if (s0 + ns < nsrc) issue(cur ^ 1, s0 + ns, min(kSpreadChunk, nsrc - s0 - ns));
+          if (s0 + ns < nsrc) issue(cur ^ 1, s0 + ns, min(SCH, nsrc - s0 - ns));
           __syncthreads();
           sp = 0;
+          ln = s_l0[0];
+          en = s_end[0];
         }
         // cell c is final
         if (active) {
@@ -516,7 +526,7 @@ __global__ void __launch_bounds__(256) k_asy_spread(
         }
         // Past the ring's last non-empty cell the next source's cell can be jumped to: all
         // accumulators are zero, so any ring position may stand for it.
-        const int nxt = sp < ns ? s_l0[sp] : INT_MAX;
+        const int nxt = sp < ns ? ln : INT_MAX;
         if (c >= last + W - 1 && nxt != INT_MAX && nxt > c + 1) c = nxt;
         else ++c;
       }
@@ -623,7 +633,10 @@ __global__ void __launch_bounds__(256) k_asy_interp(
   for (int kk = tid; kk < nk; kk += nthr) s_end[kk] = run_end(s_q0, nk, kk);
   __syncthreads();
   int kp = 0;
-  int c = s_q0[0];
+  // first cell and run end of target kp, kept in registers (loaded when kp moves, so that
+  // the loads overlap the work before the next test)
+  int qn = s_q0[0], en = s_end[0];
+  int c = qn;
   C2 gw[LPT][R];
 #pragma unroll
   for (int q = 0; q < R; ++q)
@@ -635,8 +648,12 @@ __global__ void __launch_bounds__(256) k_asy_interp(
     for (int jj = 0; jj < R; ++jj) {
       // targets whose stencil starts at cell c (ring position jj)
       for (;;) {
-        if (kp < nk && s_q0[kp] == c) {
-          const int e = s_end[kp];
+        if (kp < nk && qn == c) {
+          const int e = en;
+          if (e < nk) {
+            qn = s_q0[e];
+            en = s_end[e];
+          }
           if (tl < BT) {
 #pragma unroll 1
             for (int k = kp; k < e; ++k) {
@@ -675,10 +692,12 @@ __global__ void __launch_bounds__(256) k_asy_interp(
         if (k0 + nk < it.ke) issue(cur ^ 1, k0 + nk, min(kInterpChunk, it.ke - k0 - nk));
         __syncthreads();
         kp = 0;
+        qn = s_q0[0];
+        en = s_end[0];
       }
       if (done) break;
       // advance to the next target's cell; ring position jj + 1 stands for it
-      const int nxt = s_q0[kp];
+      const int nxt = qn;
       if (nxt == c + 1) {
         // the slot of cell c takes cell c + R (one cell ahead of the next stencil)
 #pragma unroll

@@ -1,7 +1,9 @@
 // Direct boxes: g[i,t] += sum_j c[j,t] J_nu(k_i r_j)  (src/expansions.c:78-97).
-// One Bessel value per (i, j) pair, reused across BT batch columns held in registers.
-// Tall boxes map one thread to a target; thin boxes (few targets, many sources) give each
-// target `lanes` threads that split the sources and combine with warp shuffles.
+// One Bessel value per (i, j) pair, reused across the batch columns.  k_dir (the default)
+// keeps BT columns in registers per thread: tall boxes map one thread to a target, thin boxes
+// (few targets, many sources) give each target `lanes` threads that split the sources and
+// combine with warp shuffles.  k_dir_mma (NUFHT_B200_DIR_MMA=1) evaluates tiles of Bessel
+// values and multiplies them by the coefficients on the FP64 tensor cores.
 #pragma once
 
 #include "bessel.cuh"
@@ -18,8 +20,10 @@ constexpr int kThinDirect = 16;    // asymptotic boxes this thin (sources or tar
 // coefficients of degree < kJTabCoefs in t = 2 (x - a) - 1, from J_nu at the interval's
 // Chebyshev-Gauss nodes (the exact evaluation of bessel.cuh).  J_nu and all its derivatives
 // are bounded by 1 on the real line, so the coefficients of a unit interval fall below 1e-20
-// by degree 15; evaluation is one Clenshaw sum instead of a recurrence over the order (about
-// 250 steps of Miller's algorithm at order 100 near the transition region).
+// by degree 15; evaluation is one Clenshaw sum (16 multiply-adds on 128 bytes that the
+// sorted arguments of a thread keep in L1) instead of a recurrence over the order (about 250
+// steps of Miller's algorithm at order 100 near the transition region) or Hankel's
+// expansion with up to 34 terms (order 0 from x = 17).
 constexpr int kJTabCoefs = 16;
 constexpr int kJTabMaxIntervals = 4096;
 
@@ -121,6 +125,108 @@ __global__ void __launch_bounds__(kDirThreads, 4) k_dir(
 #pragma unroll
     for (int q = 0; q < BT; ++q)
       if (t0 + q < B) atomicAdd(&gs[(size_t)(t0 + q) * ld_gs + it.i0 + ti], sgn * acc[q]);
+  }
+}
+
+// Direct boxes on the FP64 tensor cores.  Per chunk of SC sources the CTA evaluates the
+// Bessel tile J[i][s] = J_nu(k_i r_s) of its targets into shared memory (ROWS x SC = 2048
+// independent evaluations, 16 per thread, so their latency chains overlap), then adds
+// J (ROWS x SC) times c (SC x 8 NTN columns) with mma.sync.m8n8k4.f64 (DMMA) tiles: the B
+// multiply-adds per pair leave the FP64 pipe, which keeps only the Bessel evaluation.  ROWS =
+// 64 (items of up to 64 targets; warps own pairs of m-tiles) or 16 (thin boxes, up to 16
+// targets and 128 sources per chunk; the warps split the k-steps and each adds its partial
+// sums).  Shared-memory rows of SC + 4 doubles (== 4 mod 16) keep the fragment loads free of
+// bank conflicts.
+constexpr int kDirMmaTile = 2048;  // Bessel values per chunk
+constexpr int kDirMmaSources = 1024;  // sources per work item
+
+template <int ROWS>
+struct DirMmaSmem {
+  static constexpr int SC = kDirMmaTile / ROWS;  // sources per chunk
+  static constexpr int LD = SC + 4;              // row stride of J and c (doubles)
+  static constexpr size_t bytes(int BT) { return sizeof(double) * ((size_t)(ROWS + BT) * LD + SC + ROWS); }
+};
+
+template <int ROWS, int NTN>
+__global__ void __launch_bounds__(128, 4) k_dir_mma(
+    const double* __restrict__ rs, const double* __restrict__ ws, const double* __restrict__ cs,
+    int ld_cs, double* __restrict__ gs, int ld_gs, int B, const DirItem* __restrict__ items,
+    int nu2, double sgn, const double* __restrict__ jtab, int jtab_n) {
+  using S = DirMmaSmem<ROWS>;
+  constexpr int SC = S::SC, LD = S::LD;
+  constexpr int BT = 8 * NTN;
+  constexpr int MG = ROWS / 16;  // groups of two m-tiles
+  constexpr int WK = 4 / MG;     // warps sharing one group (splitting the k-steps)
+  const DirItem it = items[blockIdx.x];
+  const int t0 = blockIdx.y * BT;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int mg = warp / WK, kp = warp - mg * WK;
+  const int MT = (it.ni + 7) >> 3;  // m-tiles holding targets
+  extern __shared__ __align__(16) double dsm[];
+  double* s_J = dsm;                 // [ROWS][LD]
+  double* s_c = s_J + ROWS * LD;     // [BT][LD]: column-major tile of c
+  double* s_r = s_c + BT * LD;       // [SC]
+  double* s_k = s_r + SC;            // [ROWS]
+  for (int i = tid; i < ROWS; i += 128) s_k[i] = i < it.ni ? ws[it.i0 + i] : 0.0;
+  double acc[2][NTN][2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < NTN; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+  const int rows = MT * 8;
+  for (int s0 = 0; s0 < it.nj; s0 += SC) {
+    const int ns = min(SC, it.nj - s0);
+    __syncthreads();  // the previous chunk's tiles are consumed (and s_k is visible)
+    for (int s = tid; s < SC; s += 128) s_r[s] = s < ns ? rs[it.j0 + s0 + s] : 0.0;
+    for (int e = tid; e < BT * SC; e += 128) {
+      const int tt = e / SC, s = e - tt * SC;
+      s_c[tt * LD + s] = (s < ns && t0 + tt < B) ? cs[(size_t)(t0 + tt) * ld_cs + it.j0 + s0 + s] : 0.0;
+    }
+    __syncthreads();
+    // the Bessel tile: rows of the item's targets only (rows * SC is a multiple of 256), zeros
+    // past its targets and sources; two independent evaluations per step, both straight-line
+    // (an unused slot evaluates at x = 1 and is discarded) so that their chains overlap
+    const int nev = rows * SC;
+    for (int e = tid; e < nev; e += 256) {
+      const int e2 = e + 128;
+      const int ia = e / SC, sa = e - ia * SC;
+      const int ib = e2 / SC, sb = e2 - ib * SC;
+      const bool va = ia < it.ni && sa < ns, vb = ib < it.ni && sb < ns;
+      const double xa = va ? s_k[ia] * s_r[sa] : 1.0, xb = vb ? s_k[ib] * s_r[sb] : 1.0;
+      const double Ja = bessel_j_dir(nu2, xa, jtab, jtab_n);
+      const double Jb = bessel_j_dir(nu2, xb, jtab, jtab_n);
+      s_J[ia * LD + sa] = va ? Ja : 0.0;
+      s_J[ib * LD + sb] = vb ? Jb : 0.0;
+    }
+    __syncthreads();
+    // J x c on DMMA tiles: this warp's two m-tiles, all NTN n-tiles, its share of the k-steps
+#pragma unroll 2
+    for (int ks = kp; ks < SC / 4; ks += WK) {
+      const int k0 = ks * 4;
+      double a[2], b[NTN];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) a[q] = s_J[((mg * 2 + q) * 8 + (lane >> 2)) * LD + k0 + (lane & 3)];
+#pragma unroll
+      for (int q = 0; q < NTN; ++q) b[q] = s_c[(q * 8 + (lane >> 2)) * LD + k0 + (lane & 3)];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        if (mg * 2 + q >= MT) continue;
+#pragma unroll
+        for (int p = 0; p < NTN; ++p) dmma884(acc[q][p][0], acc[q][p][1], a[q], b[p]);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int i = (mg * 2 + q) * 8 + (lane >> 2);
+    if (i >= it.ni) continue;
+#pragma unroll
+    for (int p = 0; p < NTN; ++p)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int t = t0 + p * 8 + 2 * (lane & 3) + h;
+        if (t < B) atomicAdd(&gs[(size_t)t * ld_gs + it.i0 + i], sgn * acc[q][p][h]);
+      }
   }
 }
 

@@ -16,13 +16,6 @@
 
 namespace hankel {
 
-// d += a * b for one 8 x 8 x 4 tile: lane q holds A[q/4][q%4], B[q%4][q/4] and
-// D[q/4][2(q%4)], D[q/4][2(q%4)+1].
-__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
 
 __host__ __device__ constexpr int round8(int v) { return (v + 7) & ~7; }
 // Smallest stride >= v with stride == 4 (mod 16).

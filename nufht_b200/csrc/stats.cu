@@ -27,8 +27,11 @@ namespace hankel {
 // out[16] planning ms: work lists
 // out[17] planning ms: device tables and uploads
 // out[18] 1 when the box partition ran on the device
+// out[19] bytes of the source records (first cell, W weights, nlp factors per box source)
+// out[20] bytes of the target records (first cell, weights, nlp factors per box target)
 void plan_stats(const DevicePlan& D, double* out, int n) {
-  double s[19] = {0};
+  double s[21] = {0};
+  const double e = D.mixed_asy ? 4.0 : 8.0;  // bytes of the arithmetic type
   // Per-vector sums (entries 2-4, 8, 9) count a box with fewer expansion terms than the
   // plan's NLP in proportion (nlp / NLP), so that multiplying by NLP * B gives the work.
   for (const AsyBoxD& b : D.asyb) {
@@ -42,6 +45,9 @@ void plan_stats(const DevicePlan& D, double* out, int n) {
     s[4] += f * ni * K.W;
     s[8] += f * std::min((double)b.n2, b.n2 / K.sigma + K.W);
     s[9] += f * 5.0 * b.n2 * std::log2((double)b.n2);
+    const double we = D.mixed_asy ? ((K.W + 3) & ~3) : ((K.W + 1) & ~1);  // padded target weights
+    s[19] += nj * (4.0 + 2.0 * e * K.W + e * b.nlp);
+    s[20] += ni * (4.0 + e * we + 2.0 * e * b.nlp);
     if (K.sigma != 2.0) s[12] += 1.0;
   }
   for (const HBox& b : D.dir_boxes) s[5] += (double)(b.i1 - b.i0 + 1) * (double)(b.j1 - b.j0 + 1);
@@ -58,7 +64,7 @@ void plan_stats(const DevicePlan& D, double* out, int n) {
   s[16] = D.plan_ms[1];
   s[17] = D.plan_ms[2];
   s[18] = D.partition_on_device;
-  for (int i = 0; i < n && i < 19; ++i) out[i] = s[i];
+  for (int i = 0; i < n && i < 21; ++i) out[i] = s[i];
 }
 
 namespace {

@@ -58,9 +58,9 @@ class DevicePlan:
 
     def stats(self):
         """Work counts of the plan, its FP32 error model and its planning time
-        (nufht_b200_plan_stats, 19 values)."""
-        st = np.zeros(19)
-        L.lib().nufht_b200_plan_stats(self._h, st.ctypes.data_as(L.c_double_p), 19)
+        (nufht_b200_plan_stats, 21 values)."""
+        st = np.zeros(21)
+        L.lib().nufht_b200_plan_stats(self._h, st.ctypes.data_as(L.c_double_p), 21)
         return st
 
     def info(self):
