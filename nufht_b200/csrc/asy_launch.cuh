@@ -166,11 +166,62 @@ int launch_interp(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, int B
   }
 
 template <typename T>
+int exec_fft(const FftGroup& gr, T* grid, int B, cudaStream_t st) {
+  using C2 = typename Cplx<T>::type;
+  cufftSetStream(gr.plan, st);
+  C2* p = reinterpret_cast<C2*>(grid) + (size_t)gr.cell_off * B;
+  cufftResult fr;
+  if (sizeof(T) == 8)
+    fr = cufftExecZ2Z(gr.plan, (cufftDoubleComplex*)p, (cufftDoubleComplex*)p, CUFFT_INVERSE);
+  else
+    fr = cufftExecC2C(gr.plan, (cufftComplex*)p, (cufftComplex*)p, CUFFT_INVERSE);
+  return fr == CUFFT_SUCCESS ? 0 : NUFHT_E_CUDA;
+}
+
+// The asymptotic boxes.  Each kernel class owns disjoint grid rows, so in the concurrent
+// form every class runs its own pipeline -- spreading, the FFTs of its groups,
+// interpolation -- on its stream slot, with one fork and one join for all of them (small
+// classes and small FFT groups overlap the large ones instead of waiting at phase
+// boundaries).  With phase timing on (D.serial) the three phases run one after the other on
+// the caller's stream, so that each phase's device time can be read.
+template <typename T>
 int run_asy_t(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs, int B, cudaStream_t st,
               double sgn) {
   using C2 = typename Cplx<T>::type;
   int rc = 0;
   C2* grid = static_cast<C2*>(D.d_grid);
+  if (!D.serial) {
+    if (D.chunk_cell_end > D.chunk_cell_begin)
+      NUFHT_CUDA_TRY(cudaMemsetAsync(grid + (size_t)D.chunk_cell_begin * B, 0,
+                                     sizeof(C2) * (size_t)(D.chunk_cell_end - D.chunk_cell_begin) * B, st));
+    {
+      dim3 g((unsigned)((D.m + 31) / 32), (unsigned)((D.ldct + 31) / 32));
+      k_pack_coefficients<T><<<g, dim3(32, 8), 0, st>>>(cs, ld_cs, B, D.m, static_cast<T*>(D.d_ct), D.ldct);
+      NUFHT_LAUNCH_CHECK();
+    }
+    int used[DevicePlan::kAuxStreams];
+    int nu = 0;
+    for (int q = 0; q < DevicePlan::kAuxStreams - 2; ++q) {
+      bool any = false;
+      for (const AsyClass& K : D.classes) any = any || K.slot == q;
+      if (any) used[nu++] = 2 + q;
+    }
+    if ((rc = fork_streams(D, st, used, nu))) return rc;
+    for (int c = 0; c < (int)D.classes.size(); ++c) {
+      const AsyClass& K = D.classes[c];
+      if (K.slot < 0) continue;
+      const cudaStream_t s = D.aux[2 + K.slot];
+      if (K.nspread + K.nspreadA > 0) {
+        NUFHT_W_DISPATCH(launch_spread, T, K.W, D, K, B, s);
+        if (rc) return rc;
+      }
+      for (const FftGroup& gr : D.groups)
+        if (gr.cls == c && (rc = exec_fft<T>(gr, reinterpret_cast<T*>(grid), B, s))) return rc;
+      NUFHT_W_DISPATCH(launch_interp, T, K.W, D, K, gs, ld_gs, B, s, sgn);
+      if (rc) return rc;
+    }
+    return join_streams(D, st, used, nu);
+  }
   {
     PhaseScope ps(kPhaseSpread, st);
     if (D.chunk_cell_end > D.chunk_cell_begin)
@@ -203,16 +254,8 @@ int run_asy_t(DevicePlan& D, const double* cs, int ld_cs, double* gs, int ld_gs,
   }
   {
     PhaseScope ps(kPhaseFft, st);
-    for (const FftGroup& gr : D.groups) {
-      cufftSetStream(gr.plan, st);
-      C2* p = grid + (size_t)gr.cell_off * B;
-      cufftResult fr;
-      if (sizeof(T) == 8)
-        fr = cufftExecZ2Z(gr.plan, (cufftDoubleComplex*)p, (cufftDoubleComplex*)p, CUFFT_INVERSE);
-      else
-        fr = cufftExecC2C(gr.plan, (cufftComplex*)p, (cufftComplex*)p, CUFFT_INVERSE);
-      if (fr != CUFFT_SUCCESS) return NUFHT_E_CUDA;
-    }
+    for (const FftGroup& gr : D.groups)
+      if ((rc = exec_fft<T>(gr, reinterpret_cast<T*>(grid), B, st))) return rc;
   }
   {
     PhaseScope ps(kPhaseInterp, st);

@@ -60,6 +60,8 @@ struct SpreadItem {
 struct InterpItem { int box, ks, ke; };
 struct FftGroup {
   int n2, nbox, mode, nlp;
+  int cls;             // kernel class of the group's boxes
+  int slot;            // stream slot of that class (and of its slice of the FFT work area)
   long long cell_off;  // the group's boxes are consecutive in the workspace
   cufftHandle plan;
 };
@@ -85,6 +87,7 @@ struct AsyClass {
   int spread0, nspread;    // windowed spreading items (modes 0 and 2)
   int spreadA0, nspreadA;  // atomic spreading items (mode 1)
   int interp0, ninterp;
+  int slot;  // stream slot (0 .. kAuxStreams - 3) of the class's pipeline, -1 without boxes
 };
 
 int spread_width_for_tol(double tol);
@@ -171,6 +174,7 @@ struct DevicePlan {
   int fft_B = 0;             // batch size of the FFT plans in groups[].plan
   std::map<int, std::vector<cufftHandle>> fft_cache;  // FFT plans per batch size, one per group
   size_t fft_work_bytes = 0;
+  size_t fft_slot_bytes = 0;  // the work area holds one slice per stream slot
   // Batches (CUDA graphs) that recorded this plan's buffers and FFT plans: while pins > 0 a
   // buffer that must grow is replaced by a new allocation and the old one is kept in
   // `retired` (the graphs still use it) until the last batch lets go.
