@@ -89,13 +89,18 @@ int launch_interp_lpt(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, i
 // Terms per thread (register blocking): LPT = 2, or 1 in double precision for windows wider
 // than 10 (register budget) and for classes of at most 4 terms (so that a CTA keeps at least
 // two warps' worth of threads, NLP / LPT per column); NLP = 2 (K + 1) is even.
-// NUFHT_B200_LPT_SMALL=2 keeps two terms per thread for classes of at most 4 terms.
-inline int lpt_small() {
-  static const int v = [] {
-    const char* e = std::getenv("NUFHT_B200_LPT_SMALL");
+// NUFHT_B200_SPREAD_LPT_SMALL=2 / NUFHT_B200_INTERP_LPT_SMALL=2 keep two terms per thread for
+// the classes of at most 4 terms in spreading / interpolation.
+inline int lpt_small(bool interp) {
+  static const int vs = [] {
+    const char* e = std::getenv("NUFHT_B200_SPREAD_LPT_SMALL");
     return (e && e[0] == '2') ? 2 : 1;
   }();
-  return v;
+  static const int vi = [] {
+    const char* e = std::getenv("NUFHT_B200_INTERP_LPT_SMALL");
+    return (e && e[0] == '2') ? 2 : 1;
+  }();
+  return interp ? vi : vs;
 }
 
 template <typename T>
@@ -133,7 +138,7 @@ int build_records_t(DevicePlan& D) {
 template <typename T, int W>
 int launch_spread(DevicePlan& D, const AsyClass& K, int B, cudaStream_t st) {
   if constexpr (sizeof(T) == 8 && W > 10) return launch_spread_lpt<T, W, 1>(D, K, B, st);
-  else if (K.ac.NLP <= 4 && lpt_small() == 1) return launch_spread_lpt<T, W, 1>(D, K, B, st);
+  else if (K.ac.NLP <= 4 && lpt_small(false) == 1) return launch_spread_lpt<T, W, 1>(D, K, B, st);
   else return launch_spread_lpt<T, W, 2>(D, K, B, st);
 }
 
@@ -142,7 +147,7 @@ template <typename T, int W>
 int launch_interp(DevicePlan& D, const AsyClass& K, double* gs, int ld_gs, int B, cudaStream_t st, double sgn) {
   if (K.ninterp == 0) return 0;
   if constexpr (sizeof(T) == 8 && W > 10) return launch_interp_lpt<T, W, 1>(D, K, gs, ld_gs, B, st, sgn);
-  else if (K.ac.NLP <= 4 && lpt_small() == 1) return launch_interp_lpt<T, W, 1>(D, K, gs, ld_gs, B, st, sgn);
+  else if (K.ac.NLP <= 4 && lpt_small(true) == 1) return launch_interp_lpt<T, W, 1>(D, K, gs, ld_gs, B, st, sgn);
   else return launch_interp_lpt<T, W, 2>(D, K, gs, ld_gs, B, st, sgn);
 }
 
