@@ -304,6 +304,23 @@ struct TermBox {
   int nlp;
 };
 
+// Cost model of an asymptotic box for the term split (seconds at 32 columns on B200): per
+// source-term, target-term and cell-term, and per source and per target of the box
+// independent of its terms (record copies and the walks' control).  NUFHT_B200_SPLIT_MODEL
+// ("a,b,c,d,e" in picoseconds) replaces the fitted values (tuning).
+const double* split_model() {
+  static const std::vector<double> m = [] {
+    std::vector<double> v = {71e-12, 99e-12, 288e-12, 0.0, 0.0};
+    if (const char* e = std::getenv("NUFHT_B200_SPLIT_MODEL")) {
+      double q[5];
+      if (std::sscanf(e, "%lf,%lf,%lf,%lf,%lf", &q[0], &q[1], &q[2], &q[3], &q[4]) == 5)
+        for (int i = 0; i < 5; ++i) v[i] = q[i] * 1e-12;
+    }
+    return v;
+  }();
+  return m.data();
+}
+
 void split_by_terms(const PlanParams& P, int NLP, int W, const double* rs, const double* ws, const HBox& hb,
                     int depth, std::vector<TermBox>* out) {
   auto rref_of = [&](int j0, int j1) {
@@ -319,7 +336,8 @@ void split_by_terms(const PlanParams& P, int NLP, int W, const double* rs, const
     const double half = std::ceil(X / (M_PI / (2.0 * S)) + 0.5 * W);
     const double n2 = 2.0 * (2.0 * half + 1.0);
     const double nj = b.j1 - b.j0 + 1, ni = b.i1 - b.i0 + 1;
-    return nlp * (71e-12 * nj + 99e-12 * ni + 288e-12 * n2);
+    const double* m = split_model();
+    return nlp * (m[0] * nj + m[1] * ni + m[2] * n2) + m[3] * nj + m[4] * ni;
   };
   int nlp0 = NLP;
   const double c0 = model(hb, &nlp0);
