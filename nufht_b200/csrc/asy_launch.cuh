@@ -52,7 +52,7 @@ int launch_spread_kind(DevicePlan& D, const AsyClass& K, int item0, int nitems, 
   dim3 g((unsigned)nitems, (unsigned)L.ngy);
   k_asy_spread<T, W, LPT, TILE><<<g, L.threads, sm, st>>>(
       static_cast<const T*>(D.d_ct), D.ldct, B, static_cast<C2*>(D.d_grid), D.d_asyb, D.d_spread + item0,
-      D.d_rec_l0, static_cast<const C2*>(D.d_rec_w), static_cast<const T*>(D.d_rec_p), K.ac.NLP, L.BT, L.V_total,
+      D.d_rec_l0, static_cast<const T*>(D.d_rec_w), static_cast<const C2*>(D.d_rec_p), K.ac.NLP, L.BT, L.V_total,
       sch);
   NUFHT_LAUNCH_CHECK();
   return 0;
@@ -107,8 +107,8 @@ template <typename T>
 int build_records_t(DevicePlan& D) {
   using C2 = typename Cplx<T>::type;
   if (D.asyb.empty()) return 0;
-  const size_t b0 = sizeof(int) * (size_t)D.total_rec, b1 = sizeof(C2) * (size_t)D.total_recw,
-               b2 = sizeof(T) * (size_t)D.total_recp;
+  const size_t b0 = sizeof(int) * (size_t)D.total_rec, b1 = sizeof(T) * (size_t)D.total_recw,
+               b2 = sizeof(C2) * (size_t)D.total_recp;
   const size_t b3 = sizeof(int) * (size_t)D.total_post, b4 = sizeof(T) * (size_t)D.total_tw,
                b5 = sizeof(C2) * (size_t)D.total_tm;
   NUFHT_CUDA_TRY(cudaMalloc((void**)&D.d_rec_l0, b0));
@@ -123,8 +123,8 @@ int build_records_t(DevicePlan& D) {
     while (q1 < D.asyb.size() && D.asyb[q1].cls == D.asyb[q0].cls && q1 - q0 < 65535) ++q1;
     const AsyClass& K = D.classes[D.asyb[q0].cls];
     k_asy_records<T><<<dim3(64, (unsigned)(q1 - q0)), 256>>>(D.d_rs, D.d_asyb + q0, K.ac, K.W, D.d_corr,
-                                                              D.d_rec_l0, static_cast<C2*>(D.d_rec_w),
-                                                              static_cast<T*>(D.d_rec_p));
+                                                              D.d_rec_l0, static_cast<T*>(D.d_rec_w),
+                                                              static_cast<C2*>(D.d_rec_p));
     NUFHT_LAUNCH_CHECK();
     k_asy_target_records<T><<<dim3(64, (unsigned)(q1 - q0)), 256>>>(D.d_ws, D.d_asyb + q0, K.ac, K.W, D.d_tq0,
                                                                      static_cast<T*>(D.d_tw),

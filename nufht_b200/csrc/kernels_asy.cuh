@@ -65,10 +65,10 @@ struct AsyShape {
   int LPT, NG, BT, threads, ngy, V_total;
 };
 
-// Staged kernel weights per source (complex) and per target (real), padded so that every
-// row is read with 16-byte shared-memory loads.
+// Staged kernel weights per source and per target (real), padded so that every row is read
+// with 16-byte shared-memory loads.
 template <typename T>
-__host__ __device__ constexpr int spread_we(int W) { return sizeof(T) == 4 ? (W + 1) & ~1 : W; }
+__host__ __device__ constexpr int spread_we(int W) { return sizeof(T) == 4 ? (W + 3) & ~3 : (W + 1) & ~1; }
 template <typename T>
 __host__ __device__ constexpr int interp_we(int W) { return sizeof(T) == 4 ? (W + 3) & ~3 : (W + 1) & ~1; }
 
@@ -76,9 +76,9 @@ __host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~(siz
 
 // Shared-memory layout of k_asy_spread: two buffers (the chunk being walked and the next one,
 // filled by asynchronous copies), each with the chunk's first cells, run ends, weights (rows
-// of WE complex values), amplitude factors (rows of NLP) and coefficients (rows of BTP
-// columns); byte offsets, each region 16-byte aligned.  The host sizes the launch with the
-// same function.
+// of WE real values), amplitude factors (rows of NLP complex values) and coefficients (rows of
+// BTP columns); byte offsets, each region 16-byte aligned.  The host sizes the launch with
+// the same function.
 struct SpreadSmem {
   size_t l0, end, w, p, c, buf, total;
 };
@@ -89,8 +89,8 @@ __host__ __device__ inline SpreadSmem spread_smem(int W, int NLP, int BTP, int S
   L.l0 = 0;
   L.end = align16(L.l0 + (size_t)SCH * 4);
   L.w = align16(L.end + (size_t)SCH * 4);
-  L.p = align16(L.w + (size_t)SCH * spread_we<T>(W) * c2);
-  L.c = align16(L.p + (size_t)SCH * NLP * sizeof(T));
+  L.p = align16(L.w + (size_t)SCH * spread_we<T>(W) * sizeof(T));
+  L.c = align16(L.p + (size_t)SCH * NLP * c2);
   L.buf = align16(L.c + (size_t)SCH * BTP * sizeof(T));
   L.total = 2 * L.buf;
   return L;
@@ -192,22 +192,7 @@ __global__ void k_asy_target_records(const double* __restrict__ ws, const AsyBox
   }
 }
 
-// Weights of one source or target from shared memory (16-byte loads).
-template <int WE>
-__device__ __forceinline__ void load_weights(const float2* src, float2 (&w)[WE]) {
-  const float4* p = reinterpret_cast<const float4*>(src);
-#pragma unroll
-  for (int q = 0; q < WE / 2; ++q) {
-    float4 v = p[q];
-    w[2 * q] = make_float2(v.x, v.y);
-    w[2 * q + 1] = make_float2(v.z, v.w);
-  }
-}
-template <int WE>
-__device__ __forceinline__ void load_weights(const double2* src, double2 (&w)[WE]) {
-#pragma unroll
-  for (int q = 0; q < WE; ++q) w[q] = src[q];
-}
+// Real weights of one source or target from shared memory (16-byte loads).
 template <int WE>
 __device__ __forceinline__ void load_weights(const float* src, float (&w)[WE]) {
   const float4* p = reinterpret_cast<const float4*>(src);
@@ -248,15 +233,16 @@ __device__ __forceinline__ void grid_atomic_add(double2* p, double2 v) {
 }
 
 // Plan-time source records of stage 1 (k_asy_spread), per box and source j: first cell of
-// the kernel support at rec_off + (j - j0), W complex weights at recw_off + (j - j0) W and NLP
-// amplitude factors at recp_off + (j - j0) NLP.  The weights and the first cell follow from
-// the same FP64 position u = (r - C) / h as the cell tables; the weights are rounded to the
-// arithmetic type after the kernel value (evaluated in that type), the deconvolution factor
-// and the source phase are applied.
+// the kernel support at rec_off + (j - j0), W real weights psi(l0 + q - u) / psi-hat(l0 + q)
+// at recw_off + (j - j0) W, and NLP complex factors (rref / r)^(lp + 1/2) exp(i D (r - C))
+// at recp_off + (j - j0) NLP (the source phase is the same for all taps, so it rides with
+// the amplitude).  The weights and the first cell follow from the same FP64 position
+// u = (r - C) / h as the cell tables; the kernel value is evaluated in the arithmetic type,
+// the factors in FP64 and rounded.
 template <typename T>
 __global__ void k_asy_records(const double* __restrict__ rs, const AsyBoxD* __restrict__ boxes, AsyConst P, int W,
-                              const double* __restrict__ corr, int* __restrict__ rl0,
-                              typename Cplx<T>::type* __restrict__ rw, T* __restrict__ rp) {
+                              const double* __restrict__ corr, int* __restrict__ rl0, T* __restrict__ rw,
+                              typename Cplx<T>::type* __restrict__ rp) {
   const AsyBoxD bx = boxes[blockIdx.y];
   const int nj = bx.j1 - bx.j0 + 1;
   const T ihw = (T)(2.0 / (double)W);
@@ -269,17 +255,17 @@ __global__ void k_asy_records(const double* __restrict__ rs, const AsyBoxD* __re
     rl0[bx.rec_off + q] = l0;
     double sn, cn;
     sincos(bx.D * x, &sn, &cn);
-    const T phx = (T)cn, phy = (T)sn;
     for (int e = 0; e < W; ++e) {
       const int cell = l0 + e;
-      const T w = (cell >= -bx.half && cell <= bx.half)
-                      ? es_kernel_t((T)((double)cell - u), ihw, beta) * (T)corr[bx.corr_off + cell + bx.half]
-                      : (T)0;
-      rw[bx.recw_off + (long long)q * W + e] = cmake<T>(w * phx, w * phy);
+      rw[bx.recw_off + (long long)q * W + e] =
+          (cell >= -bx.half && cell <= bx.half)
+              ? es_kernel_t((T)((double)cell - u), ihw, beta) * (T)corr[bx.corr_off + cell + bx.half]
+              : (T)0;
     }
     const double ir = r > 0.0 ? bx.rref / r : 0.0;  // sources at r = 0 contribute nothing
     double pw = sqrt(ir);
-    for (int lp = 0; lp < bx.nlp; ++lp, pw *= ir) rp[bx.recp_off + (long long)q * bx.nlp + lp] = (T)pw;
+    for (int lp = 0; lp < bx.nlp; ++lp, pw *= ir)
+      rp[bx.recp_off + (long long)q * bx.nlp + lp] = cmake<T>((T)(pw * cn), (T)(pw * sn));
   }
 }
 
@@ -321,7 +307,7 @@ template <typename T, int W, int LPT, bool TILE>
 __global__ void __launch_bounds__(256) k_asy_spread(
     const T* __restrict__ ct, int ldct, int B, typename Cplx<T>::type* __restrict__ grid,
     const AsyBoxD* __restrict__ boxes, const SpreadItem* __restrict__ items, const int* __restrict__ rl0,
-    const typename Cplx<T>::type* __restrict__ rw, const T* __restrict__ rp, int NLP, int BT, int V_total,
+    const T* __restrict__ rw, const typename Cplx<T>::type* __restrict__ rp, int NLP, int BT, int V_total,
     int SCH) {
   using C2 = typename Cplx<T>::type;
   constexpr int WE = spread_we<T>(W);
@@ -359,22 +345,21 @@ __global__ void __launch_bounds__(256) k_asy_spread(
   auto issue = [&](int b, int s0, int ns) {
     unsigned char* base = smem_raw + (size_t)b * L.buf;
     int* d_l0 = reinterpret_cast<int*>(base + L.l0);
-    C2* d_w = reinterpret_cast<C2*>(base + L.w);
-    T* d_p = reinterpret_cast<T*>(base + L.p);
+    T* d_w = reinterpret_cast<T*>(base + L.w);
+    C2* d_p = reinterpret_cast<C2*>(base + L.p);
     T* d_c = reinterpret_cast<T*>(base + L.c);
     const int js = jr0 + s0;
     for (int s = tid; s < ns; s += nthr) cp_async4(d_l0 + s, rl0 + bx.rec_off + js + s);
-    const C2* gw = rw + bx.recw_off + (long long)js * W;
+    const T* gw = rw + bx.recw_off + (long long)js * W;
     for (int e = tid; e < ns * W; e += nthr) {
       const int s = e / W, q = e - s * W;
-      if constexpr (sizeof(T) == 4) cp_async8(d_w + s * WE + q, gw + e);
-      else cp_async16(d_w + s * WE + q, gw + e);
+      if constexpr (sizeof(T) == 4) cp_async4(d_w + s * WE + q, gw + e);
+      else cp_async8(d_w + s * WE + q, gw + e);
     }
-    // factors in pairs (NLP is even and the rows of a box start on a multiple of 4 values)
-    const T* gp = rp + bx.recp_off + (long long)js * NLP;
-    for (int e = tid; e < ns * NLP / 2; e += nthr) {
-      if constexpr (sizeof(T) == 4) cp_async8(d_p + 2 * e, gp + 2 * e);
-      else cp_async16(d_p + 2 * e, gp + 2 * e);
+    const C2* gp = rp + bx.recp_off + (long long)js * NLP;
+    for (int e = tid; e < ns * NLP; e += nthr) {
+      if constexpr (sizeof(T) == 4) cp_async8(d_p + e, gp + e);
+      else cp_async16(d_p + e, gp + e);
     }
     // coefficients: BTP columns per source in 16-byte pieces (ldct and t0 are multiples of 4;
     // pieces past the packed row are columns >= B, whose threads store nothing)
@@ -388,15 +373,15 @@ __global__ void __launch_bounds__(256) k_asy_spread(
   };
   const int* s_l0 = nullptr;
   int* s_end = nullptr;
-  const C2* s_w = nullptr;
-  const T* s_p = nullptr;
+  const T* s_w = nullptr;
+  const C2* s_p = nullptr;
   const T* s_c = nullptr;
   auto point = [&](int b) {
     unsigned char* base = smem_raw + (size_t)b * L.buf;
     s_l0 = reinterpret_cast<const int*>(base + L.l0);
     s_end = reinterpret_cast<int*>(base + L.end);
-    s_w = reinterpret_cast<const C2*>(base + L.w);
-    s_p = reinterpret_cast<const T*>(base + L.p);
+    s_w = reinterpret_cast<const T*>(base + L.w);
+    s_p = reinterpret_cast<const C2*>(base + L.p);
     s_c = reinterpret_cast<const T*>(base + L.c);
   };
 
@@ -456,23 +441,14 @@ __global__ void __launch_bounds__(256) k_asy_spread(
             if (tl < BT) {
               auto add = [&](int s) {
                 const T cv = s_c[s * BTP + tl];
-                C2 wc[WE];
-                load_weights<WE>(s_w + s * WE, wc);
-                T pv[LPT];
-                if constexpr (LPT == 2) {
-                  const typename Cplx<T>::type pp =
-                      *reinterpret_cast<const typename Cplx<T>::type*>(s_p + s * NLP + g * LPT);
-                  pv[0] = pp.x;
-                  pv[LPT - 1] = pp.y;
-                } else {
-#pragma unroll
-                  for (int u = 0; u < LPT; ++u) pv[u] = s_p[s * NLP + g * LPT + u];
-                }
+                T wt[WE];
+                load_weights<WE>(s_w + s * WE, wt);
 #pragma unroll
                 for (int u = 0; u < LPT; ++u) {
-                  const T a = cv * pv[u];
+                  const C2 pp = s_p[s * NLP + g * LPT + u];
+                  const C2 a = cmake<T>(cv * pp.x, cv * pp.y);  // complex amplitude of the source
 #pragma unroll
-                  for (int q = 0; q < W; ++q) cfma(acc[u][(jj + q) % W], wc[q], a);
+                  for (int q = 0; q < W; ++q) cfma(acc[u][(jj + q) % W], a, wt[q]);
                 }
               };
 #pragma unroll 1

@@ -46,7 +46,7 @@ void plan_stats(const DevicePlan& D, double* out, int n) {
     s[8] += f * std::min((double)b.n2, b.n2 / K.sigma + K.W);
     s[9] += f * 5.0 * b.n2 * std::log2((double)b.n2);
     const double we = D.mixed_asy ? ((K.W + 3) & ~3) : ((K.W + 1) & ~1);  // padded target weights
-    s[19] += nj * (4.0 + 2.0 * e * K.W + e * b.nlp);
+    s[19] += nj * (4.0 + e * K.W + 2.0 * e * b.nlp);
     s[20] += ni * (4.0 + e * we + 2.0 * e * b.nlp);
     if (K.sigma != 2.0) s[12] += 1.0;
   }
