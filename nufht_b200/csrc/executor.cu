@@ -696,7 +696,12 @@ void DevicePlan::build_lists() {
       for (const AsyBoxD& d : asyb)
         if (d.cls == c && d.mode == 1) dense += d.j1 - d.j0 + 1;
       if (dense > 0) {
-        const long long want = dense / (148LL * 4LL);
+        static const long long per_sm = [] {  // NUFHT_B200_CHUNK_CTAS (1..32, tuning)
+          const char* e = std::getenv("NUFHT_B200_CHUNK_CTAS");
+          const int v = e ? std::atoi(e) : 4;
+          return (long long)((v >= 1 && v <= 32) ? v : 4);
+        }();
+        const long long want = dense / (148LL * per_sm);
         chunk_src = (int)std::min<long long>(kChunkSources, std::max<long long>(256, (want + 63) / 64 * 64));
       }
     }
