@@ -343,7 +343,8 @@ def main():
     config = {"workload": workload, "nu": 0, "N": N, "M": M, "batch_per_gpu": B, "tol": tol,
               "global_batch": B * world, "precision": args.precision,
               "parallelism": "dp%d (independent column blocks per GPU, no collective)" % world,
-              "l2": "inputs larger than L2 (c and y 256 MB each, FFT workspace > 1 GB)"}
+              "l2": "inputs larger than L2 (c %d MB, y %d MB; NUFFT grids and records larger still)"
+                    % (8 * N * B // 2**20, 8 * M * B // 2**20)}
     cores = os.cpu_count() or 1
 
     if args.impl == "reference":
