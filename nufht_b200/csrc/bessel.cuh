@@ -29,35 +29,49 @@ __device__ __forceinline__ int miller_start(int M) {
   return (N + 1) & ~1;
 }
 
-// J_0(x) and J_1(x) for x >= 17 from Hankel's expansion (Abramowitz & Stegun 9.2.5-9.2.10)
+// Hankel's expansion of J_0 and J_1 for x >= 17 (Abramowitz & Stegun 9.2.5-9.2.10)
 //   J_nu(x) = sqrt(2/(pi x)) (P_nu cos chi - Q_nu sin chi),  chi = x - (nu/2 + 1/4) pi,
 //   P_nu = sum_k (-1)^k a_2k(nu) / x^2k,  Q_nu = sum_k (-1)^k a_2k+1(nu) / x^2k+1,
 //   a_0 = 1,  a_k = a_{k-1} (4 nu^2 - (2k-1)^2) / (8k),
-// with cos chi, sin chi formed from sincos(x) so that the phase keeps full precision for
-// arguments up to the largest k r of the transform.
-__device__ inline void bessel_j01_large(double x, double* J0, double* J1, bool need_j1 = true) {
-  double ix = 1.0 / x;
-  double p0 = 1.0, q0 = 0.0, p1 = 1.0, q1 = 0.0;
-  double t0 = 1.0, t1 = 1.0;
-  // Terms: at x >= 17 the terms keep decreasing past k = 34 and 34 of them leave a
-  // truncation error below 2e-16 (checked against mpmath); larger arguments need fewer
-  // (the k-th term a_k / x^k drops below 2e-17 by k = 19 at x = 25, 15 at 35, 12 at 50,
-  // 10 at 100).
-  const int nt = x >= 100.0 ? 10 : (x >= 50.0 ? 12 : (x >= 35.0 ? 15 : (x >= 25.0 ? 19 : 34)));
-#pragma unroll
+// with 34 terms (at x >= 17 the terms keep decreasing past k = 34 and these leave a
+// truncation error below 2e-16, checked against mpmath; larger arguments make the later
+// terms smaller still).  P and Q are evaluated as polynomials in y = 1/x^2 by Horner's rule
+// on coefficients computed at compile time from the recurrence: 34 multiply-adds, and
+// cos chi, sin chi formed from sincos(x) so that the phase keeps full precision for arguments
+// up to the largest k r of the transform.
+struct HankelCoefs {
+  double p[18];  // P: coefficient of y^m, terms k = 2m
+  double q[17];  // Q / (1/x): coefficient of y^m, terms k = 2m + 1
+};
+__host__ __device__ constexpr HankelCoefs hankel_coefs(double mu) {  // mu = 4 nu^2
+  HankelCoefs h{};
+  double a = 1.0;
+  h.p[0] = 1.0;
   for (int k = 1; k <= 34; ++k) {
-    if (k > nt) break;
-    const double d = (double)(2 * k - 1);
-    const double inv8k = 1.0 / (8.0 * k);  // folded at compile time
-    const double s = ((k >> 1) & 1) ? -1.0 : 1.0;  // (-1)^{floor(k/2)}
-    t0 *= (0.0 - d * d) * inv8k * ix;
-    if (k & 1) q0 = fma(s, t0, q0);
-    else p0 = fma(s, t0, p0);
-    if (need_j1) {
-      t1 *= (4.0 - d * d) * inv8k * ix;
-      if (k & 1) q1 = fma(s, t1, q1);
-      else p1 = fma(s, t1, p1);
-    }
+    const double d = 2.0 * k - 1.0;
+    a = a * (mu - d * d) / (8.0 * k);
+    const double sg = ((k >> 1) & 1) ? -1.0 : 1.0;  // (-1)^floor(k/2)
+    if (k & 1) h.q[(k - 1) / 2] = sg * a;
+    else h.p[k / 2] = sg * a;
+  }
+  return h;
+}
+
+__device__ inline void bessel_j01_large(double x, double* J0, double* J1, bool need_j1 = true) {
+  constexpr HankelCoefs h0 = hankel_coefs(0.0), h1 = hankel_coefs(4.0);
+  const double ix = 1.0 / x, y = ix * ix;
+  double p0 = h0.p[17], q0 = h0.q[16], p1 = h1.p[17], q1 = h1.q[16];
+#pragma unroll
+  for (int m = 16; m >= 0; --m) p0 = fma(p0, y, h0.p[m]);
+#pragma unroll
+  for (int m = 15; m >= 0; --m) q0 = fma(q0, y, h0.q[m]);
+  q0 *= ix;
+  if (need_j1) {
+#pragma unroll
+    for (int m = 16; m >= 0; --m) p1 = fma(p1, y, h1.p[m]);
+#pragma unroll
+    for (int m = 15; m >= 0; --m) q1 = fma(q1, y, h1.q[m]);
+    q1 *= ix;
   }
   double sn, cn;
   sincos(x, &sn, &cn);
@@ -69,7 +83,6 @@ __device__ inline void bessel_j01_large(double x, double* J0, double* J1, bool n
   *J0 = amp * (p0 * c0 - q0 * s0);
   *J1 = amp * (p1 * c1 - q1 * s1);
 }
-
 constexpr double kHankelMinX = 17.0;
 
 // J_0(x) and, when need_j1, J_1(x) for 0 <= x < 17 from the piecewise Chebyshev

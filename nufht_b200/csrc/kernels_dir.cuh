@@ -13,7 +13,7 @@ namespace hankel {
 
 constexpr int kDirThreads = 128;
 constexpr int kDirSources = 1024;  // sources per work item
-constexpr int kDirChunk = 64;      // sources staged in shared memory per round
+constexpr int kDirChunk = 128;     // sources staged in shared memory per round
 constexpr int kThinDirect = 16;    // asymptotic boxes this thin (sources or targets) are summed directly
 
 // Plan-time table of J_nu on [0, nint): on each unit interval [a, a+1) the Chebyshev
