@@ -86,11 +86,13 @@ __device__ inline void bessel_j01_large(double x, double* J0, double* J1, bool n
 constexpr double kHankelMinX = 17.0;
 
 // J_0(x) and, when need_j1, J_1(x) for 0 <= x < 17 from the piecewise Chebyshev
-// expansions of bessel_j01_table.h (unit intervals, Clenshaw summation; error below 2e-16).
+// expansions of bessel_j01_table.h (intervals of 1/kJ01PerUnit, Clenshaw summation; error
+// below 3e-16).
 __device__ inline void bessel_j01_small(double x, double* J0, double* J1, bool need_j1 = true) {
-  int a = (int)x;
+  const double xs = x * kJ01PerUnit;  // exact: a power of two
+  int a = (int)xs;
   a = a < 0 ? 0 : (a > kJ01Intervals - 1 ? kJ01Intervals - 1 : a);
-  const double t = 2.0 * (x - (double)a) - 1.0, t2 = 2.0 * t;
+  const double t = 2.0 * (xs - (double)a) - 1.0, t2 = 2.0 * t;
   const double* c0 = kJ01Cheb[0][a];
   double b1 = 0.0, b2 = 0.0;
 #pragma unroll
