@@ -31,7 +31,7 @@ def test_mixed_vs_oracle(cuda, orc, nu, tol, kind, m, n, B, seed, fp32):
     from nufht_b200 import DevicePlan
     r, k = grids(kind, m, n, seed)
     if nu == 0.5:
-        r, k = r + 1.0, k + 1.0  # half-integer method is judged away from the origin
+        r, k = r + 1.0, k + 1.0  # half-integer method is checked away from the origin
     c = np.random.default_rng(seed).standard_normal((m, B))
     p = DevicePlan(nu, r, k, tol, mixed=True)
     st = _stats(p)

@@ -16,7 +16,7 @@ def test_device_bessel_vs_mpmath(cuda, golden):
     import torch
     from nufht_b200 import _lib as L
     g = golden("bessel_golden.npz")
-    # absolute error bound 1e-14 (the transform's accuracy is judged relative to ||c||_1)
+    # absolute error bound 1e-14 (the transform's accuracy is measured relative to ||c||_1)
     for nu in np.unique(g["nu"]):
         sel = g["nu"] == nu
         x = torch.tensor(g["x"][sel], dtype=torch.float64, device=cuda)

@@ -1,10 +1,10 @@
 """The stress workload: nu = 100, N = M = 4e6, |r| from a mixture of three Gaussians (means
 200, 800, 1500; sd 50) clipped to (0, 2000], k uniform on (0, 2000], batch 64, tol 1e-8;
-forward in mixed precision (mixed="averaged": FP32 asymptotic boxes, judged on the N(0,1)
+forward in mixed precision (mixed="averaged": FP32 asymptotic boxes, checked on the N(0,1)
 columns of the workload) and the autograd backward with respect to c (the adjoint
 transform, planned and run afresh: nothing of the forward is stored but c), on one GPU.  The reference's
 tables leave K_asy = 10 empty at this order (its asymptotic boxes would get z_split = 0), so
-the plans use the extended tables, and the results are judged against the oracle's direct
+the plans use the extended tables, and the results are checked against the oracle's direct
 sums only."""
 import numpy as np
 import pytest

@@ -77,7 +77,7 @@ def test_oracle_vs_direct_sum(orc, golden):
     for name in e["names"]:
         nu, tol, B = e[name + "_meta"]
         if float(nu) == 0.5:
-            continue  # half-integer path is judged in its own test
+            continue  # half-integer path is checked in its own test
         r, k, c = e[name + "_r"], e[name + "_k"], e[name + "_c"]
         idx = np.arange(0, len(k), 37)
         d = orc.direct_sum(nu, r, k, c, idx)
