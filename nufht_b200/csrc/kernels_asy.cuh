@@ -99,19 +99,6 @@ __host__ __device__ inline SpreadSmem spread_smem(int W, int NLP, int BTP, int S
 template <typename T>
 __host__ __device__ constexpr int spread_btp(int BT) { return sizeof(T) == 4 ? (BT + 3) & ~3 : (BT + 1) & ~1; }
 
-// Asynchronous global -> shared copies (cp.async, completed by cp_async_wait_all).
-__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
-}
-__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
-}
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
 // Index one past the run of equal values that contains a[s] in the non-decreasing a[0, n).
 __device__ __forceinline__ int run_end(const int* a, int n, int s) {
   const int v = a[s];

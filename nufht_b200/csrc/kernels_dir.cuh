@@ -13,7 +13,7 @@ namespace hankel {
 
 constexpr int kDirThreads = 128;
 constexpr int kDirSources = 1024;  // sources per work item
-constexpr int kDirChunk = 128;     // sources staged in shared memory per round
+constexpr int kDirChunk = 64;      // sources per shared-memory stage (two stages in flight)
 constexpr int kThinDirect = 16;    // asymptotic boxes this thin (sources or targets) are summed directly
 
 // Plan-time table of J_nu on [0, nint): on each unit interval [a, a+1) the Chebyshev
@@ -84,38 +84,56 @@ __global__ void __launch_bounds__(kDirThreads, 4) k_dir(
   const int ti = tid / L, lane = tid - ti * L;
   const bool valid = ti < it.ni;
   const double k = valid ? ws[it.i0 + ti] : 0.0;
-  __shared__ double s_r[kDirChunk];
-  __shared__ double s_c[BT * kDirChunk];  // [column][source]
+  // Two stages of kDirChunk sources: radii and the BT columns of c ([column][source]), filled
+  // by asynchronous copies while the CTA sums the other stage.
+  __shared__ __align__(16) double s_r[2][kDirChunk];
+  __shared__ __align__(16) double s_c[2][BT * kDirChunk];
   double acc[BT];
 #pragma unroll
   for (int q = 0; q < BT; ++q) acc[q] = 0.0;
+  auto stage = [&](int b, int s0) {
+    const int ns = min(kDirChunk, it.nj - s0);
+    for (int s = tid; s < kDirChunk; s += kDirThreads) {
+      if (s < ns) cp_async8(&s_r[b][s], rs + it.j0 + s0 + s);
+      else s_r[b][s] = 0.0;
+    }
+    for (int e = tid; e < kDirChunk * BT; e += kDirThreads) {
+      const int tt = e / kDirChunk, s = e - tt * kDirChunk;
+      if (s < ns && t0 + tt < B) cp_async8(&s_c[b][e], cs + (size_t)(t0 + tt) * ld_cs + it.j0 + s0 + s);
+      else s_c[b][e] = 0.0;
+    }
+    cp_async_commit();
+  };
+  stage(0, 0);
+  int b = 0;
   for (int s0 = 0; s0 < it.nj; s0 += kDirChunk) {
     const int ns = min(kDirChunk, it.nj - s0);
-    for (int s = tid; s < ns; s += kDirThreads) s_r[s] = rs[it.j0 + s0 + s];
-    for (int e = tid; e < kDirChunk * BT; e += kDirThreads) {
-      int tt = e / kDirChunk, s = e - tt * kDirChunk;
-      s_c[e] = (s < ns && t0 + tt < B) ? cs[(size_t)(t0 + tt) * ld_cs + it.j0 + s0 + s] : 0.0;
-    }
-    __syncthreads();
+    cp_async_wait_all();  // this thread's copies of stage b have landed
+    __syncthreads();      // all copies of stage b visible; stage b ^ 1 no longer read
+    if (s0 + kDirChunk < it.nj) stage(b ^ 1, s0 + kDirChunk);
+    const double* cr = s_r[b];
+    const double* cc = s_c[b];
     if (valid) {
-      // Two independent Bessel evaluations per step for instruction-level parallelism.
+      // Two independent Bessel evaluations per step for instruction-level parallelism.  The
+      // stage length is a multiple of 2 L, so each thread visits its sources in the same
+      // order whatever the stage length.
       int s = lane;
       for (; s + L < ns; s += 2 * L) {
-        double Ja = bessel_j_dir(nu2, k * s_r[s], jtab, jtab_n);
-        double Jb = bessel_j_dir(nu2, k * s_r[s + L], jtab, jtab_n);
+        double Ja = bessel_j_dir(nu2, k * cr[s], jtab, jtab_n);
+        double Jb = bessel_j_dir(nu2, k * cr[s + L], jtab, jtab_n);
 #pragma unroll
         for (int q = 0; q < BT; ++q) {
-          acc[q] = fma(s_c[q * kDirChunk + s], Ja, acc[q]);
-          acc[q] = fma(s_c[q * kDirChunk + s + L], Jb, acc[q]);
+          acc[q] = fma(cc[q * kDirChunk + s], Ja, acc[q]);
+          acc[q] = fma(cc[q * kDirChunk + s + L], Jb, acc[q]);
         }
       }
       if (s < ns) {
-        double J = bessel_j_dir(nu2, k * s_r[s], jtab, jtab_n);
+        double J = bessel_j_dir(nu2, k * cr[s], jtab, jtab_n);
 #pragma unroll
-        for (int q = 0; q < BT; ++q) acc[q] = fma(s_c[q * kDirChunk + s], J, acc[q]);
+        for (int q = 0; q < BT; ++q) acc[q] = fma(cc[q * kDirChunk + s], J, acc[q]);
       }
     }
-    __syncthreads();
+    b ^= 1;
   }
   for (int off = L >> 1; off > 0; off >>= 1) {
 #pragma unroll
