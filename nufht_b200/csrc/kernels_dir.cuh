@@ -14,6 +14,7 @@ namespace hankel {
 constexpr int kDirThreads = 128;
 constexpr int kDirSources = 1024;  // sources per work item
 constexpr int kDirChunk = 64;      // sources per shared-memory stage (two stages in flight)
+static_assert(kDirChunk % 64 == 0, "a stage must hold whole pairs of steps of up to 32 lanes");
 constexpr int kThinDirect = 16;    // asymptotic boxes this thin (sources or targets) are summed directly
 
 // Plan-time table of J_nu on [0, nint): on each unit interval [a, a+1) the Chebyshev
